@@ -1,0 +1,409 @@
+#!/usr/bin/env python
+"""Benchmark of the GATLAS hot path on B200.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step is one pass of the hot path over one batch of synthetic input:
+  * headline  : SGEMM at FP32 accuracy, C = A·B, M = N = K = 8192, FP32
+                operands uniform[-1,1) (the precision-sweep workload), on the
+                FP32-accurate engine (split-BF16 tensor cores when built,
+                otherwise the SIMT kernel);
+  * secondary : the memory-bound pair at full size, SGEMV y = A·x and
+                y = A^T·x with A 16384^2 and SAXPY y = 0.5·x + y with n = 2^28,
+                reported in GB/s against measured HBM bandwidth.
+Every operand is larger than the 126 MB L2, so no flush is needed between
+timed iterations.  Timing uses CUDA events on the launching stream, max over
+ranks; N > 1 runs independent replicas (weak scaling, no collective on the
+data path).  Rank 0 prints one JSON line.
+
+--impl reference times the reference's own algorithm on the host cores: the
+reference's OpenCL kernels need an OpenCL platform that this machine lacks,
+so its CPU implementation is the oracle port (oracle/), a bounded sample of
+the same workload per step.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+M_GEMM = 8192
+N_GEMV = 16384
+N_SAXPY = 1 << 28
+METRIC = "SGEMM TFLOP/s at FP32 accuracy (3xBF16 TC vs SIMT FP32); GEMV GB/s; p99 lat"
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"]),
+                "bf16_tflops_sustained": float(d.get("bf16_tflops_sustained", d["bf16_tflops"])),
+                "source": "measured"}
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0,
+                "source": "fallback"}
+
+
+# nominal FP32 SIMT peak: 148 SMs x 128 FP32 lanes x 2 flop x 1.965 GHz
+FP32_SIMT_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines: list[str] = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self._t = threading.Thread(target=self._read, daemon=True)
+        self._t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+
+def _dist_init(n_gpus: int):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return rank, world, local
+
+
+def _barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def _max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# our implementation
+# ---------------------------------------------------------------------------
+
+def _fp32_engine(g):
+    for eng in ("tc_split3",):
+        if g.matmul_supported(eng):
+            return eng
+    return "buffer"
+
+
+def _timed(fn, steps, warmup, world, stream):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    _barrier(world)
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(steps):
+        fn()
+    stop.record(stream)
+    torch.cuda.synchronize()
+    _barrier(world)
+    return start.elapsed_time(stop) / steps  # ms per step
+
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    import gatlas_b200 as g
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    peaks = _peaks()
+    engine = _fp32_engine(g)
+
+    # ---- headline: SGEMM 8192^3 --------------------------------------------
+    M = N = K = M_GEMM
+    A = torch.empty(M * K, dtype=torch.float32, device=dev)
+    B = torch.empty(K * N, dtype=torch.float32, device=dev)
+    C = torch.empty(M * N, dtype=torch.float32, device=dev)
+    g.fill(A, "uniform", seed=1 + rank)
+    g.fill(B, "uniform", seed=2 + rank)
+    ws_bytes = g.matmul_workspace_size(M, N, K, engine)
+    ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
+    launches_per_step = 1 if engine == "buffer" else 3
+
+    def step():
+        g.matmul(A, B, M, N, K, C=C, engine=engine, workspace=ws if ws_bytes else None)
+
+    step()
+    torch.cuda.synchronize()
+    fro, refn, mx, _ = g.residual(A, B, C, M, N, K)
+    err = fro / refn
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    ms = _timed(step, args.steps, args.warmup, world, stream)
+    clocks = sampler.stop()
+    ms_max = _max_over_ranks(ms, world)
+    flops = 2.0 * M * N * K
+    value = world * flops / (ms_max * 1e-3) / 1e12
+
+    # kernel-only time of the dominant kernel (the GEMM launch itself)
+    if engine == "buffer":
+        dom_ms = ms
+        roofline = {"bound": "fp32_simt", "achieved": flops / (dom_ms * 1e-3) / 1e12,
+                    "peak": FP32_SIMT_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+                    "peak_source": "nominal (148 SMs x 128 FP32 lanes x 2 x 1.965 GHz); "
+                                   "no measured FP32 SIMT peak on this pool",
+                    "traffic": None}
+        roofline["frac"] = roofline["achieved"] / roofline["peak"]
+    else:
+        dom_ms = ms
+        pk = peaks["bf16_tflops"]
+        ach = 3 * flops / (dom_ms * 1e-3) / 1e12
+        roofline = {"bound": "tensor", "achieved": ach, "peak": pk, "unit": "TFLOP/s",
+                    "frac": ach / pk, "traffic": None,
+                    "peak_source": f"{peaks['source']} bf16 (burst); 3 BF16 products per FP32 MAC"}
+
+    # ---- e2e through the C ABI with host buffers -----------------------------
+    hA = torch.empty(M * K, dtype=torch.float32, pin_memory=True)
+    hB = torch.empty(K * N, dtype=torch.float32, pin_memory=True)
+    hC = torch.empty(M * N, dtype=torch.float32, pin_memory=True)
+    hA.copy_(A, non_blocking=False)
+    hB.copy_(B, non_blocking=False)
+
+    def e2e_step():
+        A.copy_(hA, non_blocking=True)
+        B.copy_(hB, non_blocking=True)
+        g.matmul(A, B, M, N, K, C=C, engine=engine, workspace=ws if ws_bytes else None)
+        hC.copy_(C, non_blocking=True)
+
+    e2e_steps = max(2, min(args.steps, 10))
+    e2e_ms = _max_over_ranks(_timed(e2e_step, e2e_steps, 1, world, stream), world)
+    e2e = {"value": world * flops / (e2e_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
+           "h2d_bytes_per_step": 2 * M * K * 4, "d2h_bytes_per_step": M * N * 4,
+           "ms_per_step": e2e_ms}
+    del hA, hB, hC
+
+    # ---- secondary: memory-bound pair ----------------------------------------
+    secondary = {}
+    del C
+    Ag = torch.empty(N_GEMV * N_GEMV, dtype=torch.float32, device=dev)
+    xg = torch.empty(N_GEMV, dtype=torch.float32, device=dev)
+    yg = torch.empty(N_GEMV, dtype=torch.float32, device=dev)
+    g.fill(Ag, "uniform", seed=3)
+    g.fill(xg, "uniform", seed=4)
+    gemv_bytes = 4.0 * (N_GEMV * N_GEMV + 2 * N_GEMV)
+    for ta in (0, 1):
+        for eng in ("buffer", "image"):
+            try:
+                g.matvec(Ag, xg, N_GEMV, N_GEMV, y=yg, trans_a=ta, engine=eng)
+            except g.GatlasError:
+                continue
+            t = _timed(lambda: g.matvec(Ag, xg, N_GEMV, N_GEMV, y=yg, trans_a=ta, engine=eng),
+                       max(args.steps, 10), 3, world, stream)
+            secondary[f"sgemv_{'At' if ta else 'A'}x_{eng}_gbs"] = gemv_bytes / (t * 1e-3) / 1e9
+    del Ag, xg, yg
+    xs = torch.empty(N_SAXPY, dtype=torch.float32, device=dev)
+    ys = torch.empty(N_SAXPY, dtype=torch.float32, device=dev)
+    g.fill(xs, "uniform", seed=5)
+    g.fill(ys, "uniform", seed=6)
+    for eng in ("buffer", "image"):
+        t = _timed(lambda: g.saxpy(0.5, xs, ys, out=ys, engine=eng), max(args.steps, 10), 3,
+                   world, stream)
+        secondary[f"saxpy_{eng}_gbs"] = 12.0 * N_SAXPY / (t * 1e-3) / 1e9
+    for k in list(secondary):
+        secondary[k.replace("_gbs", "_hbm_frac")] = secondary[k] / peaks["hbm_gbs"]
+    del xs, ys
+
+    faults = g.device_faults()
+    cpu = cpu_baseline(args.cpu_seconds) if (rank == 0 and world == 1 and not args.no_cpu) else None
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded uniform[-1,1) FP32 operands generated on the device)",
+        "config": {"workload": "sgemm_fp32_accurate_8192", "m": M, "n": N, "k": K,
+                   "engine": engine, "layout": "row-major, no transposes",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "operands larger than L2; no flush"},
+        "error_vs_fp64": {"normwise": err, "max_abs": mx},
+        "e2e": e2e, "roofline": roofline, "secondary": secondary,
+        "gpu_launches": launches_per_step * args.steps, "clocks": clocks,
+        "device_faults": faults,
+    }
+    if cpu:
+        out["cpu_baseline"] = cpu
+    return out
+
+
+# ---------------------------------------------------------------------------
+# CPU legs (the oracle port of the reference's algorithm)
+# ---------------------------------------------------------------------------
+
+def _cpu_rows_for(seconds: float, threads: int) -> int:
+    """Rows of C whose computation takes about `seconds` on the host cores
+    (from a 16-row pilot), a multiple of 16 in [16, 8192]."""
+    import oracle
+    K = N = M_GEMM
+    A = oracle.uniform(16 * K, seed=1)
+    B = oracle.uniform(K * N, seed=2)
+    t0 = time.perf_counter()
+    oracle.matmul_tiled(A, B, 16, N, K, tile_m=16, tile_n=64, threads=threads)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    rows = int(16 * seconds / dt) // 16 * 16
+    return max(16, min(M_GEMM, rows))
+
+
+def cpu_baseline(seconds: float) -> dict:
+    """The reference's buffer-kernel algorithm (one tile per work group, fused
+    mad chain over k) on the host cores, on a bounded sample of the 8192^3
+    workload: the first rows of C, sized to about `seconds` of CPU work."""
+    import oracle
+    threads = oracle.max_threads()
+    K = N = M_GEMM
+    rows = _cpu_rows_for(seconds, threads)
+    A = oracle.uniform(rows * K, seed=1)
+    B = oracle.uniform(K * N, seed=2)
+    t0 = time.perf_counter()
+    oracle.matmul_tiled(A, B, rows, N, K, tile_m=128, tile_n=64, threads=threads)
+    dt = time.perf_counter() - t0
+    flops = 2.0 * rows * N * K
+    return {"value": flops / dt / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": "port",
+            "sample": f"{rows} of 8192 rows of C of the 8192^3 SGEMM "
+                      f"({flops / 1e9:.0f} GFLOP in {dt:.1f} s)"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    import oracle
+    threads = oracle.max_threads()
+    K = N = M_GEMM
+    # each step a bounded sample sized so the whole run takes a few minutes
+    per_step_s = max(1.0, min(8.0, 150.0 / max(1, args.steps + args.warmup)))
+    rows = _cpu_rows_for(per_step_s, threads)
+    A = oracle.uniform(rows * K, seed=1)
+    B = oracle.uniform(K * N, seed=2)
+    for _ in range(min(args.warmup, 1)):
+        oracle.matmul_tiled(A, B, min(rows, 16), N, K, tile_m=16, tile_n=64, threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.matmul_tiled(A, B, rows, N, K, tile_m=128, tile_n=64, threads=threads)
+        times.append(time.perf_counter() - t0)
+    dt = sum(times) / len(times)
+    flops = 2.0 * rows * N * K
+    v = flops / dt / 1e12
+    return {
+        "metric": METRIC, "value": v, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "impl": "reference",
+        "data": "synthetic (seeded uniform[-1,1) FP32 operands)",
+        "config": {"workload": "sgemm_fp32_accurate_8192", "m": M_GEMM, "n": M_GEMM, "k": M_GEMM,
+                   "engine": "the reference's buffer-kernel algorithm on the host cores "
+                             "(oracle port; the reference needs an OpenCL platform)"},
+        "cpu_baseline": {"value": v, "unit": "TFLOP/s", "cores": threads, "kind": "port",
+                         "sample": f"{rows} of 8192 rows of C of the 8192^3 SGEMM per step"},
+        "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="CPU work in the cpu_baseline sample")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        res = run_reference(args, rank, world)
+        if res is not None:
+            print(json.dumps(res), flush=True)
+        return
+    rank, world, local = _dist_init(args.gpus)
+    res = run_ours(args, rank, world, local)
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,245 @@
+"""gatlas_b200: B200-native GEMM / GEMV / SAXPY hot path of GATLAS.
+
+Python binding of the C ABI declared in include/gatlas.h (ctypes over the
+in-tree gatlas_b200/lib/libgatlas_b200.so).  Device memory, streams and
+tensors come from PyTorch; every computation runs in the library's CUDA
+kernels.  There is no CPU fallback: if the library is missing, the import of
+any op raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libgatlas_b200.so")
+
+GATLAS_OK = 0
+ERR_INVALID, ERR_CUDA, ERR_UNSUPPORTED, ERR_TIMEOUT, ERR_NOMEM, ERR_CHECK, ERR_STATE = (
+    -1, -2, -3, -4, -5, -6, -7)
+
+ENGINES = {"buffer": 0, "image": 1, "tc_bf16": 2, "tc_split3": 3, "tc_split6": 4, "tc_fp8": 5}
+DISTS = {"uniform": 0, "pow2": 1, "const": 2}
+
+
+class GatlasError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"gatlas status {status}: {message}")
+        self.status = status
+
+
+class MatmulDesc(ctypes.Structure):
+    _fields_ = [("engine", ctypes.c_int32), ("gemm", ctypes.c_int32),
+                ("trans_a", ctypes.c_int32), ("trans_b", ctypes.c_int32),
+                ("m", ctypes.c_uint64), ("n", ctypes.c_uint64), ("k", ctypes.c_uint64),
+                ("lda", ctypes.c_uint64), ("ldb", ctypes.c_uint64), ("ldc", ctypes.c_uint64),
+                ("batch", ctypes.c_uint64), ("stride_a", ctypes.c_uint64),
+                ("stride_b", ctypes.c_uint64), ("stride_c", ctypes.c_uint64),
+                ("alpha", ctypes.c_double), ("beta", ctypes.c_double),
+                ("group_h", ctypes.c_uint32), ("group_w", ctypes.c_uint32),
+                ("block_h", ctypes.c_uint32), ("block_w", ctypes.c_uint32),
+                ("vector_length", ctypes.c_uint32), ("extra", ctypes.c_uint32)]
+
+
+class MatvecDesc(ctypes.Structure):
+    _fields_ = [("engine", ctypes.c_int32), ("gemv", ctypes.c_int32),
+                ("trans_a", ctypes.c_int32), ("reserved0", ctypes.c_int32),
+                ("m", ctypes.c_uint64), ("n", ctypes.c_uint64), ("lda", ctypes.c_uint64),
+                ("batch", ctypes.c_uint64), ("stride_a", ctypes.c_uint64),
+                ("stride_x", ctypes.c_uint64), ("stride_y", ctypes.c_uint64),
+                ("alpha", ctypes.c_double), ("beta", ctypes.c_double)]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Loads the in-tree library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -j8` at the repository "
+                           "root (or __graft_entry__.build())")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, sz, i32, u64 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_uint64
+    L.gatlas_version.restype = i32
+    L.gatlas_status_string.restype = ctypes.c_char_p
+    L.gatlas_status_string.argtypes = [i32]
+    L.gatlas_last_error.restype = sz
+    L.gatlas_last_error.argtypes = [ctypes.c_char_p, sz]
+    L.gatlas_saxpy_f32.argtypes = [i32, sz, ctypes.c_float, vp, vp, vp, vp]
+    L.gatlas_saxpy_f64.argtypes = [i32, sz, ctypes.c_double, vp, vp, vp, vp]
+    L.gatlas_matvec_workspace_size.argtypes = [ctypes.POINTER(MatvecDesc)]
+    L.gatlas_matvec_workspace_size.restype = sz
+    for n in ("gatlas_matvec_f32", "gatlas_matvec_f64"):
+        getattr(L, n).argtypes = [ctypes.POINTER(MatvecDesc), vp, vp, vp, vp, sz, vp]
+    L.gatlas_matmul_workspace_size.argtypes = [ctypes.POINTER(MatmulDesc)]
+    L.gatlas_matmul_workspace_size.restype = sz
+    for n in ("gatlas_matmul_f32", "gatlas_matmul_f64"):
+        getattr(L, n).argtypes = [ctypes.POINTER(MatmulDesc), vp, vp, vp, vp, sz, vp]
+    L.gatlas_matmul_supported.argtypes = [i32, ctypes.POINTER(MatmulDesc)]
+    L.gatlas_fill_f32.argtypes = [vp, sz, i32, u64, u64, ctypes.c_float, vp]
+    L.gatlas_fill_f64.argtypes = [vp, sz, i32, u64, u64, ctypes.c_double, vp]
+    L.gatlas_matmul_residual_f32.argtypes = [ctypes.POINTER(MatmulDesc), vp, vp, vp,
+                                             ctypes.POINTER(ctypes.c_double), vp]
+    L.gatlas_device_faults.argtypes = [ctypes.POINTER(ctypes.c_int), i32]
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    buf = ctypes.create_string_buffer(512)
+    lib().gatlas_last_error(buf, 512)
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int) -> int:
+    if status != GATLAS_OK:
+        raise GatlasError(status, last_error() or lib().gatlas_status_string(status).decode())
+    return status
+
+
+# ---------------------------------------------------------------------------
+# torch helpers
+# ---------------------------------------------------------------------------
+
+def _torch():
+    import torch
+    return torch
+
+
+def _ptr(t):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _stream(stream=None):
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def _engine(engine) -> int:
+    return ENGINES[engine] if isinstance(engine, str) else int(engine)
+
+
+def _require_cuda(*ts):
+    for t in ts:
+        if t is not None and not t.is_cuda:
+            raise ValueError("gatlas_b200 ops take CUDA tensors")
+
+
+# ---------------------------------------------------------------------------
+# ops
+# ---------------------------------------------------------------------------
+
+def saxpy(alpha, x, y, out=None, engine="buffer", stream=None):
+    """out = fma(alpha, x, y) elementwise (out may be y for in-place)."""
+    torch = _torch()
+    _require_cuda(x, y, out)
+    if out is None:
+        out = torch.empty_like(y)
+    n = x.numel()
+    assert y.numel() == n and out.numel() == n
+    assert x.dtype == y.dtype == out.dtype
+    if x.dtype == torch.float32:
+        fn = lib().gatlas_saxpy_f32
+    elif x.dtype == torch.float64:
+        fn = lib().gatlas_saxpy_f64
+    else:
+        raise TypeError(f"saxpy: unsupported dtype {x.dtype}")
+    check(fn(_engine(engine), n, float(alpha), _ptr(x), _ptr(y), _ptr(out), _stream(stream)))
+    return out
+
+
+def matvec_desc(M, N, trans_a=False, gemv=False, alpha=1.0, beta=0.0, engine="buffer",
+                lda=0, batch=1, stride_a=0, stride_x=0, stride_y=0) -> MatvecDesc:
+    return MatvecDesc(engine=_engine(engine), gemv=int(bool(gemv)), trans_a=int(bool(trans_a)),
+                      reserved0=0, m=M, n=N, lda=lda, batch=batch, stride_a=stride_a,
+                      stride_x=stride_x, stride_y=stride_y, alpha=alpha, beta=beta)
+
+
+def matvec(A, x, M, N, y=None, trans_a=False, gemv=False, alpha=1.0, beta=0.0,
+           engine="buffer", batch=1, workspace=None, stream=None):
+    """y = A·x (or alpha·A·x + beta·y).  A is flat: trans_a=False → M×N
+    row-major; trans_a=True → column-major (N rows of M)."""
+    torch = _torch()
+    _require_cuda(A, x, y)
+    if y is None:
+        y = torch.zeros(batch * M, dtype=A.dtype, device=A.device)
+    d = matvec_desc(M, N, trans_a, gemv, alpha, beta, engine, batch=batch)
+    fn = lib().gatlas_matvec_f32 if A.dtype == torch.float32 else lib().gatlas_matvec_f64
+    ws = _ptr(workspace)
+    wsb = 0 if workspace is None else workspace.numel() * workspace.element_size()
+    check(fn(ctypes.byref(d), _ptr(A), _ptr(x), _ptr(y), ws, wsb, _stream(stream)))
+    return y
+
+
+def matvec_workspace_size(M, N, trans_a=False, batch=1) -> int:
+    d = matvec_desc(M, N, trans_a, batch=batch)
+    return int(lib().gatlas_matvec_workspace_size(ctypes.byref(d)))
+
+
+def matmul_desc(M, N, K, trans_a=False, trans_b=False, gemm=False, alpha=1.0, beta=0.0,
+                engine="buffer", tile=None, batch=1, lda=0, ldb=0, ldc=0,
+                stride_a=0, stride_b=0, stride_c=0) -> MatmulDesc:
+    t = tuple(tile or ())
+    gh, gw, bh, bw, vl, x = t + (0,) * (6 - len(t))
+    return MatmulDesc(engine=_engine(engine), gemm=int(bool(gemm)), trans_a=int(bool(trans_a)),
+                      trans_b=int(bool(trans_b)), m=M, n=N, k=K, lda=lda, ldb=ldb, ldc=ldc,
+                      batch=batch, stride_a=stride_a, stride_b=stride_b, stride_c=stride_c,
+                      alpha=alpha, beta=beta, group_h=gh, group_w=gw, block_h=bh, block_w=bw,
+                      vector_length=vl, extra=x)
+
+
+def matmul(A, B, M, N, K, C=None, trans_a=False, trans_b=False, gemm=False, alpha=1.0,
+           beta=0.0, engine="buffer", tile=None, batch=1, workspace=None, stream=None):
+    """C = op(A)·op(B) (or alpha·op(A)·op(B) + beta·C) on flat tensors in the
+    reference's layouts (see include/gatlas.h)."""
+    torch = _torch()
+    _require_cuda(A, B, C)
+    if C is None:
+        C = torch.empty(batch * M * N, dtype=A.dtype, device=A.device)
+    d = matmul_desc(M, N, K, trans_a, trans_b, gemm, alpha, beta, engine, tile, batch)
+    fn = lib().gatlas_matmul_f32 if A.dtype == torch.float32 else lib().gatlas_matmul_f64
+    ws = _ptr(workspace)
+    wsb = 0 if workspace is None else workspace.numel() * workspace.element_size()
+    check(fn(ctypes.byref(d), _ptr(A), _ptr(B), _ptr(C), ws, wsb, _stream(stream)))
+    return C
+
+
+def matmul_supported(engine="buffer", tile=None, trans_a=False, trans_b=False, double=False):
+    d = matmul_desc(1, 1, 1, trans_a, trans_b, engine=engine, tile=tile)
+    return bool(lib().gatlas_matmul_supported(int(double), ctypes.byref(d)))
+
+
+def matmul_workspace_size(M, N, K, engine, trans_a=False, trans_b=False, batch=1) -> int:
+    d = matmul_desc(M, N, K, trans_a, trans_b, engine=engine, batch=batch)
+    return int(lib().gatlas_matmul_workspace_size(ctypes.byref(d)))
+
+
+def fill(t, dist="uniform", seed=0, offset=0, value=0.0, stream=None):
+    """Seeded device-side fill (same stream as the host oracle's generators)."""
+    torch = _torch()
+    _require_cuda(t)
+    fn = lib().gatlas_fill_f32 if t.dtype == torch.float32 else lib().gatlas_fill_f64
+    check(fn(_ptr(t), t.numel(), DISTS[dist] if isinstance(dist, str) else int(dist), seed,
+             offset, float(value), _stream(stream)))
+    return t
+
+
+def residual(A, B, C, M, N, K, trans_a=False, trans_b=False, alpha=1.0, stream=None):
+    """FP64 residual of C against op(A)·op(B) computed on the GPU in double:
+    (||C-Cref||_F, ||Cref||_F, max|C-Cref|, sum|C-Cref|)."""
+    d = matmul_desc(M, N, K, trans_a, trans_b, gemm=alpha != 1.0, alpha=alpha)
+    out = (ctypes.c_double * 4)()
+    check(lib().gatlas_matmul_residual_f32(ctypes.byref(d), _ptr(A), _ptr(B), _ptr(C), out,
+                                           _stream(stream)))
+    return tuple(out)
+
+
+def device_faults(clear=True) -> int:
+    v = ctypes.c_int(0)
+    check(lib().gatlas_device_faults(ctypes.byref(v), int(clear)))
+    return v.value

@@ -1,0 +1,71 @@
+// Per-device fault word and scratch cache.
+#include <mutex>
+
+#include "common.cuh"
+#include "device_state.cuh"
+
+namespace gatlas {
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+int *g_fault[kMaxDevices] = {nullptr};
+void *g_scratch[kMaxDevices] = {nullptr};
+size_t g_scratch_bytes[kMaxDevices] = {0};
+
+int current_device() {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return -1;
+    return dev;
+}
+}  // namespace
+
+int *device_fault_word() {
+    const int dev = current_device();
+    if (dev < 0) return nullptr;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_fault[dev]) {
+        int *p = nullptr;
+        if (cudaMalloc(&p, sizeof(int)) != cudaSuccess) return nullptr;
+        if (cudaMemset(p, 0, sizeof(int)) != cudaSuccess) {
+            cudaFree(p);
+            return nullptr;
+        }
+        g_fault[dev] = p;
+    }
+    return g_fault[dev];
+}
+
+void *device_scratch(size_t bytes) {
+    const int dev = current_device();
+    if (dev < 0) return nullptr;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_scratch_bytes[dev] < bytes) {
+        if (g_scratch[dev]) {
+            cudaDeviceSynchronize();
+            cudaFree(g_scratch[dev]);
+            g_scratch[dev] = nullptr;
+            g_scratch_bytes[dev] = 0;
+        }
+        // round up to 2 MiB so that slowly growing requests do not reallocate often
+        const size_t want = (bytes + ((size_t)2 << 20) - 1) & ~(((size_t)2 << 20) - 1);
+        void *p = nullptr;
+        if (cudaMalloc(&p, want) != cudaSuccess) return nullptr;
+        g_scratch[dev] = p;
+        g_scratch_bytes[dev] = want;
+    }
+    return g_scratch[dev];
+}
+
+}  // namespace gatlas
+
+extern "C" int gatlas_device_faults(int *flags, int clear) {
+    int *w = gatlas::device_fault_word();
+    if (!w) return gatlas::set_error(GATLAS_ERR_CUDA, "fault word unavailable");
+    int v = 0;
+    cudaError_t e = cudaMemcpy(&v, w, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return gatlas::set_error(GATLAS_ERR_CUDA, "read fault word: %s", cudaGetErrorString(e));
+    if (clear && v) cudaMemset(w, 0, sizeof(int));
+    if (flags) *flags = v;
+    return GATLAS_OK;
+}

@@ -1,0 +1,34 @@
+// Per-device library state: the fault word that bounded device waits set when
+// they give up, and cached scratch buffers for callers that pass no workspace.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+namespace gatlas {
+
+// Bits of the per-device fault word (read with gatlas_device_faults()).
+enum FaultCode : int {
+    kFaultSaxpyBulkWait = 1 << 0,
+    kFaultGemvTmaWait = 1 << 1,
+    kFaultGemmTmaWait = 1 << 2,
+    kFaultTcProducerWait = 1 << 3,
+    kFaultTcMmaWait = 1 << 4,
+    kFaultTcEpilogueWait = 1 << 5,
+};
+
+// Device pointer to the current device's fault word (allocated and zeroed on
+// first use); nullptr if the allocation failed.
+int *device_fault_word();
+
+// Current device's cached scratch buffer of at least `bytes` (grown on demand,
+// never shrunk).  nullptr on failure.  Not safe to grow during graph capture.
+void *device_scratch(size_t bytes);
+
+#ifdef __CUDACC__
+__device__ __forceinline__ void report_fault(int *word, int code) {
+    if (word) atomicOr(word, code);
+}
+#endif
+
+}  // namespace gatlas

@@ -1,0 +1,163 @@
+/*
+ * gatlas_b200 — C ABI of the B200-native GEMM / GEMV / SAXPY hot path.
+ *
+ * Plain C: no C++ or torch types cross this boundary.  Every entry point
+ * returns an int status (GATLAS_OK == 0, negative on error) unless stated
+ * otherwise; gatlas_last_error() returns the calling thread's last message.
+ * Device pointers are caller-owned CUDA device memory on the current device;
+ * `stream` is a cudaStream_t passed as void* (NULL = the legacy default stream).
+ *
+ * Each declaration cites the reference (GATLAS) interface it replaces.  The
+ * reference has no C ABI: its plugin boundary is the C++ virtual interface
+ * KernelInterface (GatlasBenchmark.hpp:28-58) plus the KernelBase* setters,
+ * and its device boundary is clEnqueueNDRangeKernel on generated OpenCL C.
+ */
+#ifndef GATLAS_B200_H
+#define GATLAS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status ------------------------------------------------------------ */
+#define GATLAS_OK 0
+#define GATLAS_ERR_INVALID (-1)     /* invalid argument or parameter point */
+#define GATLAS_ERR_CUDA (-2)        /* CUDA runtime / driver error */
+#define GATLAS_ERR_UNSUPPORTED (-3) /* valid point with no kernel built for it */
+#define GATLAS_ERR_TIMEOUT (-4)     /* a bounded device wait expired */
+#define GATLAS_ERR_NOMEM (-5)       /* allocation failed */
+#define GATLAS_ERR_CHECK (-6)       /* output check failed */
+#define GATLAS_ERR_STATE (-7)       /* call out of order (e.g. run before set_args) */
+
+int gatlas_version(void);
+const char *gatlas_status_string(int status);
+/* Copies the calling thread's last error message; returns its length. */
+size_t gatlas_last_error(char *buf, size_t len);
+
+/* ---- enums ------------------------------------------------------------- */
+/* Engines.  BUFFER and IMAGE are the reference's two kernel families
+ * ("matmulbuffer", "matmulimage", ...); on B200 the image family loads its
+ * operands with TMA tensor-map / bulk copies instead of texture fetches.
+ * The TC_* engines are tcgen05 tensor-core contractions (no reference
+ * counterpart): BF16 operands with FP32 accumulation, FP32 operands split
+ * into BF16 pieces (3 or 6 products), FP8 E4M3 with FP32 block scales. */
+enum {
+    GATLAS_ENGINE_BUFFER = 0,
+    GATLAS_ENGINE_IMAGE = 1,
+    GATLAS_ENGINE_TC_BF16 = 2,
+    GATLAS_ENGINE_TC_SPLIT3 = 3,
+    GATLAS_ENGINE_TC_SPLIT6 = 4,
+    GATLAS_ENGINE_TC_FP8 = 5
+};
+
+enum { GATLAS_DIST_UNIFORM = 0, GATLAS_DIST_POW2 = 1, GATLAS_DIST_CONST = 2 };
+
+/* ---- SAXPY --------------------------------------------------------------
+ * z[i] = fma(alpha, x[i], y[i]) for i < n; z may alias y (in place).
+ * Replaces KernelSaxpyBuffer<float,VL> / KernelSaxpyImage<float,4>
+ * (KernelSaxpyBuffer.hpp:143-225, KernelSaxpyImage.hpp:148-233), whose
+ * generated kernels compute Z = mad(alpha, X, Y).  Results are bit-exact
+ * against a per-element fmaf. */
+int gatlas_saxpy_f32(int engine, size_t n, float alpha, const float *x, const float *y, float *z,
+                     void *stream);
+int gatlas_saxpy_f64(int engine, size_t n, double alpha, const double *x, const double *y,
+                     double *z, void *stream);
+
+/* ---- GEMV ---------------------------------------------------------------
+ * y[p] = A[p]·x[p] (gemv == 0) or alpha·A[p]·x[p] + beta·y[p] (gemv == 1)
+ * for p < batch.  trans_a == 0: A is M×N row-major (element (i,j) at
+ * A[i*lda + j], lda >= N); trans_a == 1: A is stored column-major (element
+ * (i,j) at A[j*lda + i], lda >= M), the reference's transposeA layout
+ * (KernelMatvecBuffer.hpp:128-131).  Replaces KernelMatvecBuffer<float,VL>
+ * and KernelMatvecImage<float,4> (KernelMatvecBuffer.hpp:180-325,
+ * KernelMatvecImage.hpp:188-295).  Deterministic: the summation order
+ * depends only on (M, N, engine) and the device's SM count.
+ * `workspace` may be NULL, in which case the library uses an internal
+ * per-device buffer; gatlas_matvec_workspace_size() gives the bytes needed. */
+typedef struct gatlas_matvec_desc {
+    int32_t engine;  /* GATLAS_ENGINE_BUFFER or GATLAS_ENGINE_IMAGE */
+    int32_t gemv;
+    int32_t trans_a;
+    int32_t reserved0;
+    uint64_t m, n, lda;
+    uint64_t batch;                      /* packedCalc; 0 means 1 */
+    uint64_t stride_a, stride_x, stride_y; /* elements between instances; 0 = dense */
+    double alpha, beta;
+} gatlas_matvec_desc;
+
+size_t gatlas_matvec_workspace_size(const gatlas_matvec_desc *d);
+int gatlas_matvec_f32(const gatlas_matvec_desc *d, const float *A, const float *x, float *y,
+                      void *workspace, size_t workspace_bytes, void *stream);
+int gatlas_matvec_f64(const gatlas_matvec_desc *d, const double *A, const double *x, double *y,
+                      void *workspace, size_t workspace_bytes, void *stream);
+
+/* ---- GEMM ---------------------------------------------------------------
+ * C[p] = op(A[p])·op(B[p]) (gemm == 0) or alpha·op(A[p])·op(B[p]) + beta·C[p]
+ * (gemm == 1; C is not read when beta == 0).  Layouts follow the reference
+ * (KernelMatmulBuffer.hpp:131-136): trans_a == 0 → A is M×K row-major
+ * (lda >= K); trans_a == 1 → A stored K×M row-major (lda >= M); trans_b == 0
+ * → B is K×N row-major (ldb >= N); trans_b == 1 → B stored N×K row-major
+ * (ldb >= K); C is M×N row-major (ldc >= N).  ld* == 0 means dense.
+ * The SIMT tile is the reference's work-group × inner-blocking point
+ * (KernelBaseMatmul.hpp:85-140): a group_h × group_w thread block computes a
+ * (group_h·block_h) × (group_w·block_w) tile; vector_length is the width of
+ * the global loads; extra is the reference's extra parameter (recorded, no
+ * effect on the arithmetic).  Zeros select the tuned default.
+ * Replaces KernelMatmulBuffer<SCALAR,VL> and KernelMatmulImage<SCALAR,VL>
+ * (KernelMatmulBuffer.hpp:174-342, KernelMatmulImage.hpp:192-313).
+ * SIMT engines accumulate k = 0..K-1 as one fused multiply-add chain per
+ * element, bit-exact against a sequential fmaf chain. */
+typedef struct gatlas_matmul_desc {
+    int32_t engine;
+    int32_t gemm;
+    int32_t trans_a, trans_b;
+    uint64_t m, n, k;
+    uint64_t lda, ldb, ldc;
+    uint64_t batch;                       /* packedCalc; 0 means 1 */
+    uint64_t stride_a, stride_b, stride_c; /* elements between instances; 0 = dense */
+    double alpha, beta;
+    uint32_t group_h, group_w, block_h, block_w, vector_length, extra;
+} gatlas_matmul_desc;
+
+/* Bytes of scratch the engine needs (split / quantised operand copies for the
+ * TC_* engines, 0 for SIMT).  workspace may be NULL: the library then uses an
+ * internal per-device buffer. */
+size_t gatlas_matmul_workspace_size(const gatlas_matmul_desc *d);
+int gatlas_matmul_f32(const gatlas_matmul_desc *d, const float *A, const float *B, float *C,
+                      void *workspace, size_t workspace_bytes, void *stream);
+int gatlas_matmul_f64(const gatlas_matmul_desc *d, const double *A, const double *B, double *C,
+                      void *workspace, size_t workspace_bytes, void *stream);
+/* 1 if a compiled kernel exists for (scalar 0=float/1=double, desc), else 0. */
+int gatlas_matmul_supported(int scalar, const gatlas_matmul_desc *d);
+
+/* ---- data generation and residuals ---------------------------------------
+ * Seeded device-side generators (splitmix64 counter streams shared with the
+ * host oracle): uniform [-1,1), sign·2^e (e in [-8,8]) or a constant. */
+int gatlas_fill_f32(float *out, size_t n, int dist, uint64_t seed, uint64_t offset, float value,
+                    void *stream);
+int gatlas_fill_f64(double *out, size_t n, int dist, uint64_t seed, uint64_t offset, double value,
+                    void *stream);
+
+/* FP64 residual of a float result against an FP64 reference product computed
+ * on the GPU (the paranoid check, OCLAppUtil.hpp:212-264, moved to the device):
+ * out[0] = ||C - Cref||_F, out[1] = ||Cref||_F, out[2] = max |C - Cref|,
+ * out[3] = sum |C - Cref| (the reference's absdiff), with Cref = op(A)·op(B)
+ * accumulated in double.  Only the dense, batch == 1 layout is accepted. */
+int gatlas_matmul_residual_f32(const gatlas_matmul_desc *d, const float *A, const float *B,
+                               const float *C, double *out_host, void *stream);
+
+/* ---- device faults ------------------------------------------------------
+ * Kernels that wait on asynchronous copies (mbarrier waits) give up after a
+ * bounded number of polls, set a bit in the current device's fault word and
+ * return instead of hanging.  Reads the word after synchronising the device;
+ * clears it when `clear` is non-zero.  No reference counterpart (the
+ * reference detects hangs only through its journal, GatlasBenchmark.cpp:178-289). */
+int gatlas_device_faults(int *flags, int clear);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GATLAS_B200_H */

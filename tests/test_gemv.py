@@ -1,0 +1,105 @@
+"""GEMV parity: within the normwise tolerance 4*N*u of the FP64 oracle, exact
+on the reference's test pattern (c == N)."""
+import os
+
+import numpy as np
+import pytest
+
+import gatlas_b200 as g
+import oracle
+
+pytestmark = pytest.mark.gpu
+GOLDEN = np.load(os.path.join(os.path.dirname(__file__), "golden", "oracle_small.npz"))
+U32 = 2.0 ** -24
+
+
+def _gpu(cuda, a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to(cuda)
+
+
+def _matvec(cuda, A, x, M, N, ta, engine="buffer", gemv=False, yin=None, alpha=1.0, beta=0.0,
+            batch=1):
+    import torch
+    y = _gpu(cuda, yin) if yin is not None else torch.zeros(batch * M, dtype=torch.float32, device=cuda)
+    g.matvec(_gpu(cuda, A), _gpu(cuda, x), M, N, y=y, trans_a=ta, gemv=gemv, alpha=alpha,
+             beta=beta, engine=engine, batch=batch)
+    torch.cuda.synchronize()
+    return y.cpu().numpy()
+
+
+@pytest.mark.parametrize("ta", [0, 1])
+def test_golden_fixture(cuda, ta):
+    M, N = (int(v) for v in GOLDEN["mv_dims"])
+    y = _matvec(cuda, GOLDEN[f"mv_t{ta}_A"], GOLDEN[f"mv_t{ta}_x"], M, N, ta)
+    assert oracle.normwise_error(y, GOLDEN[f"mv_t{ta}_f64"]) <= 4 * N * U32
+    y = _matvec(cuda, GOLDEN[f"mv_t{ta}_A"], GOLDEN[f"mv_t{ta}_x"], M, N, ta, gemv=True,
+                yin=GOLDEN[f"mv_t{ta}_yin"], alpha=0.5, beta=2.0)
+    assert oracle.normwise_error(y, GOLDEN[f"mv_t{ta}_gemv_f64"]) <= 4 * N * U32
+
+
+@pytest.mark.parametrize("ta", [0, 1])
+@pytest.mark.parametrize("M,N", [(64, 64), (1024, 4096), (4096, 1024), (16384, 512)])
+def test_known_answer_c_equals_n(cuda, ta, M, N):
+    y = _matvec(cuda, np.ones(M * N, np.float32), np.ones(N, np.float32), M, N, ta)
+    assert oracle.check_pattern(y, float(N))
+
+
+@pytest.mark.parametrize("ta", [0, 1])
+@pytest.mark.parametrize("M,N", [(1, 1), (1, 37), (37, 1), (33, 65), (127, 129), (1000, 1001),
+                                 (2048, 3072), (4099, 257)])
+def test_tolerance_vs_f64(cuda, ta, M, N):
+    A = oracle.uniform(M * N, seed=M * 7 + N)
+    x = oracle.uniform(N, seed=N * 3 + 1)
+    y = _matvec(cuda, A, x, M, N, ta)
+    ref = oracle.matvec(A, x, M, N, ta, mode=oracle.F64)
+    assert oracle.normwise_error(y, ref) <= 4 * N * U32
+
+
+@pytest.mark.parametrize("ta", [0, 1])
+def test_gemv_alpha_beta_and_batch(cuda, ta):
+    M, N, P = 300, 500, 3
+    A = oracle.uniform(P * M * N, seed=1)
+    x = oracle.uniform(P * N, seed=2)
+    yin = oracle.uniform(P * M, seed=3)
+    y = _matvec(cuda, A, x, M, N, ta, gemv=True, yin=yin, alpha=-0.5, beta=1.5, batch=P)
+    ref = oracle.matvec(A, x, M, N, ta, mode=oracle.F64, gemv=1, cin=yin, alpha=-0.5, beta=1.5,
+                        packed=P)
+    assert oracle.normwise_error(y, ref) <= 4 * N * U32
+
+
+@pytest.mark.parametrize("ta", [0, 1])
+def test_deterministic(cuda, ta):
+    M, N = 2048, 2048
+    A = oracle.uniform(M * N, seed=5)
+    x = oracle.uniform(N, seed=6)
+    y1 = _matvec(cuda, A, x, M, N, ta)
+    y2 = _matvec(cuda, A, x, M, N, ta)
+    assert np.array_equal(y1, y2)
+
+
+def test_empty_inner_dimension(cuda):
+    # N == 0: y = alpha*0 + beta*y
+    yin = oracle.uniform(64, seed=9)
+    for ta in (0, 1):
+        y = _matvec(cuda, np.zeros(1, np.float32), np.zeros(1, np.float32), 64, 0, ta, gemv=True,
+                    yin=yin, alpha=2.0, beta=0.5)
+        assert np.array_equal(y, (yin * np.float32(0.5)).astype(np.float32))
+
+
+@pytest.mark.parametrize("ta", [0, 1])
+def test_full_size_16384(cuda, ta):
+    # BASELINE size: A 16384^2 (1 GiB); checked against FP64 on 256 sampled rows
+    import torch
+    M = N = 16384
+    A = torch.empty(M * N, dtype=torch.float32, device=cuda)
+    x = torch.empty(N, dtype=torch.float32, device=cuda)
+    g.fill(A, "uniform", seed=11)
+    g.fill(x, "uniform", seed=12)
+    y = g.matvec(A, x, M, N, trans_a=ta)
+    torch.cuda.synchronize()
+    rows = np.random.default_rng(0).choice(M, 256, replace=False)
+    A64 = A.view(N, M).double() if ta else A.view(M, N).double()
+    ref = (A64[:, rows].T if ta else A64[rows]) @ x.double()
+    err = torch.linalg.norm(y[rows].double() - ref) / torch.linalg.norm(ref)
+    assert float(err) <= 4 * N * U32

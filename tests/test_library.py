@@ -1,0 +1,65 @@
+"""The C-ABI library loads and exports every entry point include/*.h declares
+(CPU; no compute calls)."""
+import ctypes
+import glob
+import os
+import re
+
+import gatlas_b200 as g
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(gatlas_[a-z0-9_]+)\s*\(", text):
+            names.add(m.group(1))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = g.lib()
+    names = declared_symbols()
+    assert len(names) >= 15
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_status_strings_and_version():
+    lib = g.lib()
+    assert lib.gatlas_version() >= 100
+    assert lib.gatlas_status_string(0) == b"ok"
+    assert lib.gatlas_status_string(-3) == b"unsupported parameter point"
+
+
+def test_argument_errors_need_no_gpu():
+    lib = g.lib()
+    # null descriptors and pointers are rejected before any CUDA call
+    assert lib.gatlas_matmul_f32(None, None, None, None, None, 0, None) == g.ERR_INVALID
+    assert "null descriptor" in g.last_error()
+    assert lib.gatlas_matvec_f32(None, None, None, None, None, 0, None) == g.ERR_INVALID
+    assert lib.gatlas_saxpy_f32(0, 16, ctypes.c_float(1.0), None, None, None, None) == g.ERR_INVALID
+    assert lib.gatlas_saxpy_f32(7, 0, ctypes.c_float(1.0), None, None, None, None) == 0  # n == 0 is a no-op
+    d = g.matmul_desc(8, 8, 8, engine=9)
+    assert lib.gatlas_matmul_f32(ctypes.byref(d), ctypes.c_void_p(16), ctypes.c_void_p(16),
+                                 ctypes.c_void_p(16), None, 0, None) == g.ERR_INVALID
+
+
+def test_compiled_simt_points_cover_the_tuning_grid():
+    # work group {8,16}^2 x blocking {4,8}^2 x vector width {1,2,4}, no transposes
+    for gh in (8, 16):
+        for gw in (8, 16):
+            for bh in (4, 8):
+                for bw in (4, 8):
+                    for vl in (1, 2, 4):
+                        assert g.matmul_supported("buffer", (gh, gw, bh, bw, vl))
+    assert not g.matmul_supported("buffer", (10, 10, 7, 4, 4))
+
+
+def test_workspace_queries():
+    assert g.matvec_workspace_size(16384, 16384, trans_a=False) == 0
+    assert g.matvec_workspace_size(16384, 16384, trans_a=True) > 0
+    assert g.matmul_workspace_size(1024, 1024, 1024, "buffer") == 0
