@@ -1,16 +1,469 @@
-// Tensor-core (tcgen05) matmul engines.
+// Tensor-core (tcgen05) matmul engines: BF16 operands with FP32 accumulation,
+// and FP32-accurate contractions of FP32 operands split into BF16 pieces.
+//
+// No reference counterpart: the reference's matmul kernels are SIMT mad
+// chains (KernelMatmulBuffer.hpp:302-321).  These engines compute the same
+// C = op(A)·op(B) (alpha/beta, packed batches, all four layouts) on the
+// 5th-generation tensor cores:
+//
+//  1. split pass: every FP32 operand element x is split into BF16 pieces
+//     (x = hi + lo + r with hi = bf16(x), lo = bf16(x - hi), |r| <= 2^-17|x|;
+//     three pieces hi + mid + lo represent x exactly) written K-major
+//     ([rows][Kp], Kp = K rounded up to 8, zero padded), transposing the
+//     operands whose stored layout is not K-major;
+//  2. contraction: one CTA per 128 x 256 tile of C, 128 threads.  Warp 0
+//     lane 0 streams BK = 32 slices of every piece of A and B with 3-D TMA
+//     tensor-map loads (64-byte swizzle) into a multi-stage mbarrier ring;
+//     warp 1 lane 0 issues tcgen05.mma kind::f16 (M=128, N=256, K=16) for
+//     each product of pieces (hi·hi, hi·lo, lo·hi for 3 products; the six
+//     leading products of three pieces for 6), accumulating in FP32 in TMEM
+//     (256 columns); after the last slice all four warps read the
+//     accumulator back with tcgen05.ld 32x32b and apply
+//     C = fma(alpha, acc, beta*C).
+// Every mbarrier wait is bounded in wall time; a timeout sets the device
+// fault word, stops the pipeline, drains the copies in flight and frees TMEM.
+#include <cuda.h>
+#include <cuda_bf16.h>
+
 #include "../common.cuh"
+#include "../device_state.cuh"
+#include "../tcgen05.cuh"
+#include "../tma.hpp"
 #include "gemm_engines.hpp"
 
 namespace gatlas {
+namespace tcg {
 
-int matmul_tc(const gatlas_matmul_desc *, const Geometry &, const float *, const float *, float *, void *,
-              size_t, cudaStream_t) {
-    return set_error(GATLAS_ERR_UNSUPPORTED, "matmul: tensor-core engines not built yet");
+constexpr int BM = 128, BN = 256, BK = 32;
+constexpr int kThreads = 128;
+constexpr uint32_t kTmemCols = 256;
+constexpr uint32_t kRowBytes = BK * 2;        // 64 B rows -> 64-byte swizzle
+constexpr uint32_t kSBO = 8 * kRowBytes;      // 8-row core-matrix groups
+constexpr uint32_t kATile = BM * kRowBytes;   // 8 KiB
+constexpr uint32_t kBTile = BN * kRowBytes;   // 16 KiB
+constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s bound on any single wait
+
+// MODE 0: one BF16 piece, one product; 1: two pieces, three products;
+// 2: three pieces, six products.
+template <int MODE>
+struct Mode;
+template <>
+struct Mode<0> {
+    static constexpr int NP = 1, NPROD = 1, STAGES = 8;
+    __device__ static constexpr int pa(int) { return 0; }
+    __device__ static constexpr int pb(int) { return 0; }
+};
+template <>
+struct Mode<1> {
+    static constexpr int NP = 2, NPROD = 3, STAGES = 4;
+    // hi*hi, hi*lo, lo*hi
+    __device__ static constexpr int pa(int j) { return j == 2 ? 1 : 0; }
+    __device__ static constexpr int pb(int j) { return j == 1 ? 1 : 0; }
+};
+template <>
+struct Mode<2> {
+    static constexpr int NP = 3, NPROD = 6, STAGES = 3;
+    // hi*hi, hi*mid, mid*hi, mid*mid, hi*lo, lo*hi
+    __device__ static constexpr int pa(int j) { return j == 2 || j == 3 ? 1 : (j == 5 ? 2 : 0); }
+    __device__ static constexpr int pb(int j) { return j == 1 || j == 3 ? 1 : (j == 4 ? 2 : 0); }
+};
+
+template <int MODE>
+struct Layout {
+    static constexpr int NP = Mode<MODE>::NP;
+    static constexpr int STAGES = Mode<MODE>::STAGES;
+    static constexpr uint32_t STAGE_BYTES = NP * (kATile + kBTile);
+    static constexpr uint32_t SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + alignment slack
+};
+
+struct Params {
+    float *C;
+    int64_t M, N, ldc, stride_c;
+    int kblocks;
+    float alpha, beta;
+    int gemm;
+    int *fault;
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 1)
+    tc_gemm_kernel(const __grid_constant__ CUtensorMap ta0, const __grid_constant__ CUtensorMap ta1,
+                   const __grid_constant__ CUtensorMap ta2, const __grid_constant__ CUtensorMap tb0,
+                   const __grid_constant__ CUtensorMap tb1, const __grid_constant__ CUtensorMap tb2,
+                   Params p) {
+    using L = Layout<MODE>;
+    using MD = Mode<MODE>;
+    constexpr int S = L::STAGES;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    __shared__ __align__(8) uint64_t full[S], empty[S], accf;
+    __shared__ uint32_t tmem_base;
+    __shared__ volatile int abort_flag;
+    __shared__ int kb_issued, kb_consumed;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN, z = blockIdx.z;
+    const CUtensorMap *tA[3] = {&ta0, &ta1, &ta2};
+    const CUtensorMap *tB[3] = {&tb0, &tb1, &tb2};
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&accf, 1);
+        fence_mbarrier_init();
+        abort_flag = 0;
+        kb_issued = 0;
+        kb_consumed = 0;
+        for (int i = 0; i < MD::NP; ++i) {
+            prefetch_tmap(tA[i]);
+            prefetch_tmap(tB[i]);
+        }
+    }
+    if (warp == 0) {
+        tc::tmem_alloc(&tmem_base, kTmemCols);
+        tc::tmem_relinquish();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_base;
+
+    auto a_tile = [&](int s, int piece) { return smem + s * L::STAGE_BYTES + piece * kATile; };
+    auto b_tile = [&](int s, int piece) { return smem + s * L::STAGE_BYTES + MD::NP * kATile + piece * kBTile; };
+
+    if (warp == 0) {
+      if (lane == 0) {
+        // ---- TMA producer ----
+        int kb = 0;
+        for (; kb < p.kblocks; ++kb) {
+            const int s = kb % S;
+            const uint32_t ph = (uint32_t)(kb / S) & 1u;
+            if (!tc::wait_timed(&empty[s], ph ^ 1u, kWaitNs, &abort_flag)) {
+                if (!abort_flag) report_fault(p.fault, kFaultTcProducerWait);
+                abort_flag = 1;
+                break;
+            }
+            mbar_arrive_expect_tx(&full[s], L::STAGE_BYTES);
+            for (int i = 0; i < MD::NP; ++i) {
+                tma_load_3d(a_tile(s, i), tA[i], kb * BK, m0, z, &full[s]);
+                tma_load_3d(b_tile(s, i), tB[i], kb * BK, n0, z, &full[s]);
+            }
+        }
+        kb_issued = kb;
+      }
+      __syncwarp();
+    } else if (warp == 1) {
+      if (lane == 0) {
+        // ---- MMA issuer ----
+        constexpr uint32_t idesc = tc::idesc_bf16_f32(BM, BN);
+        int kb = 0;
+        for (; kb < p.kblocks; ++kb) {
+            const int s = kb % S;
+            const uint32_t ph = (uint32_t)(kb / S) & 1u;
+            if (!tc::wait_timed(&full[s], ph, kWaitNs, &abort_flag)) {
+                if (!abort_flag) report_fault(p.fault, kFaultTcMmaWait);
+                abort_flag = 1;
+                break;
+            }
+            tc::fence_after_sync();
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk) {
+#pragma unroll
+                for (int j = 0; j < MD::NPROD; ++j) {
+                    const uint32_t a_addr = smem_u32(a_tile(s, MD::pa(j))) + kk * 32;
+                    const uint32_t b_addr = smem_u32(b_tile(s, MD::pb(j))) + kk * 32;
+                    tc::mma_bf16(tmem, tc::smem_desc_kmajor(a_addr, kSBO, tc::kSwizzle64B),
+                                 tc::smem_desc_kmajor(b_addr, kSBO, tc::kSwizzle64B), idesc,
+                                 (kb | kk | j) != 0 ? 1u : 0u);
+                }
+            }
+            tc::commit_to(&empty[s]);
+        }
+        kb_consumed = kb;
+        tc::commit_to(&accf);  // fires when every MMA issued above has completed
+      }
+      __syncwarp();
+    }
+
+    // ---- epilogue: TMEM -> registers -> C ----
+    const bool acc_ready = tc::wait_timed(&accf, 0, 2 * kWaitNs, nullptr);
+    if (!acc_ready && threadIdx.x == 0) report_fault(p.fault, kFaultTcEpilogueWait);
+    tc::fence_after_sync();
+    __syncthreads();
+    if (acc_ready && !abort_flag) {
+        const int64_t row = (int64_t)m0 + warp * 32 + lane;
+        float *crow = p.C + (int64_t)z * p.stride_c + row * p.ldc;
+        const bool vec_ok = (p.ldc % 4 == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0) &&
+                            (p.stride_c % 4 == 0);
+#pragma unroll 1
+        for (int c = 0; c < BN / 32; ++c) {
+            uint32_t r[32];
+            tc::tmem_ld_32x32b_x32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * 32), r);
+            tc::tmem_ld_wait();
+            if (row < p.M) {
+                const int64_t col0 = (int64_t)n0 + c * 32;
+                float v[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const float acc = __uint_as_float(r[j]);
+                    if (p.gemm) {
+                        const int64_t col = col0 + j;
+                        const float bc = (p.beta == 0.0f || col >= p.N) ? 0.0f : p.beta * crow[col];
+                        v[j] = __fmaf_rn(p.alpha, acc, bc);
+                    } else {
+                        v[j] = acc;
+                    }
+                }
+                if (vec_ok && col0 + 31 < p.N) {
+#pragma unroll
+                    for (int j = 0; j < 32; j += 4)
+                        *reinterpret_cast<float4 *>(crow + col0 + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        if (col0 + j < p.N) crow[col0 + j] = v[j];
+                }
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    // after an abort: wait (bounded) for copies still landing in shared memory
+    if (threadIdx.x == 0 && abort_flag) {
+        for (int kb = kb_consumed; kb < kb_issued; ++kb)
+            tc::wait_timed(&full[kb % S], (uint32_t)(kb / S) & 1u, kWaitNs, nullptr);
+    }
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, kTmemCols);
 }
 
-int tc_supported(const gatlas_matmul_desc *) { return 0; }
+// ---------------------------------------------------------------------------
+// split pass: FP32 -> NP BF16 pieces, K-major [batch][rows][Kp]
+// ---------------------------------------------------------------------------
+template <int NP>
+__device__ __forceinline__ void split_value(float x, __nv_bfloat16 (&out)[3]) {
+    const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+    out[0] = hi;
+    if constexpr (NP >= 2) {
+        const float r1 = x - __bfloat162float(hi);  // exact
+        const __nv_bfloat16 mid = __float2bfloat16_rn(r1);
+        out[1] = mid;
+        if constexpr (NP >= 3) {
+            const float r2 = r1 - __bfloat162float(mid);  // exact
+            out[2] = __float2bfloat16_rn(r2);
+        }
+    }
+}
 
-size_t tc_workspace_bytes(const gatlas_matmul_desc *, const Geometry &) { return 0; }
+struct SplitArgs {
+    const float *src;
+    int64_t rows, K, Kp, ld, src_stride;  // src element (r,k): src[r*ld + k] (direct) or src[k*ld + r] (transposed)
+    __nv_bfloat16 *out[3];
+    int64_t piece_stride;                 // elements per instance in each piece: rows*Kp
+};
+
+template <int NP>
+__global__ void __launch_bounds__(256) split_direct_kernel(SplitArgs a) {
+    const int64_t quads_per_row = a.Kp / 4;
+    const int64_t total = a.rows * quads_per_row;
+    const int64_t z = blockIdx.y;
+    const float *src = a.src + z * a.src_stride;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = q / quads_per_row, k = (q % quads_per_row) * 4;
+        __nv_bfloat16 pcs[4][3];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const float x = (k + e < a.K) ? src[r * a.ld + k + e] : 0.0f;
+            split_value<NP>(x, pcs[e]);
+        }
+#pragma unroll
+        for (int i = 0; i < NP; ++i) {
+            __nv_bfloat162 v0 = __halves2bfloat162(pcs[0][i], pcs[1][i]);
+            __nv_bfloat162 v1 = __halves2bfloat162(pcs[2][i], pcs[3][i]);
+            uint2 u;
+            u.x = *reinterpret_cast<uint32_t *>(&v0);
+            u.y = *reinterpret_cast<uint32_t *>(&v1);
+            *reinterpret_cast<uint2 *>(a.out[i] + z * a.piece_stride + r * a.Kp + k) = u;
+        }
+    }
+}
+
+// Source stored K x rows (element (r,k) at src[k*ld + r]); 32 x 32 tiles
+// transposed through shared memory so both the reads and the writes coalesce.
+template <int NP>
+__global__ void __launch_bounds__(256) split_transpose_kernel(SplitArgs a) {
+    __shared__ float tile[32][33];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+    const int64_t r0 = (int64_t)blockIdx.x * 32, k0 = (int64_t)blockIdx.y * 32;
+    const int64_t z = blockIdx.z;
+    const float *src = a.src + z * a.src_stride;
+#pragma unroll
+    for (int j = 0; j < 32; j += 8) {
+        const int64_t k = k0 + ty + j, r = r0 + tx;
+        tile[ty + j][tx] = (k < a.K && r < a.rows) ? src[k * a.ld + r] : 0.0f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 32; j += 8) {
+        const int64_t r = r0 + ty + j, k = k0 + tx;
+        if (r < a.rows && k < a.Kp) {
+            __nv_bfloat16 pcs[3];
+            split_value<NP>(tile[tx][ty + j], pcs);
+#pragma unroll
+            for (int i = 0; i < NP; ++i) a.out[i][z * a.piece_stride + r * a.Kp + k] = pcs[i];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+struct Plan {
+    int mode;  // 0 bf16, 1 split3, 2 split6
+    int np;
+    int64_t Kp;
+    size_t a_piece_bytes, b_piece_bytes, total;
+};
+
+static inline size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+static bool make_plan(const gatlas_matmul_desc *d, const Geometry &g, Plan *pl) {
+    switch (d->engine) {
+        case GATLAS_ENGINE_TC_BF16: pl->mode = 0; pl->np = 1; break;
+        case GATLAS_ENGINE_TC_SPLIT3: pl->mode = 1; pl->np = 2; break;
+        case GATLAS_ENGINE_TC_SPLIT6: pl->mode = 2; pl->np = 3; break;
+        default: return false;
+    }
+    pl->Kp = (int64_t)round_up((size_t)(g.K > 0 ? g.K : 1), 8);
+    pl->a_piece_bytes = round_up((size_t)g.batch * (size_t)g.M * (size_t)pl->Kp * 2, 1024);
+    pl->b_piece_bytes = round_up((size_t)g.batch * (size_t)g.N * (size_t)pl->Kp * 2, 1024);
+    pl->total = pl->np * (pl->a_piece_bytes + pl->b_piece_bytes);
+    return true;
+}
+
+static int launch_split(int np, bool transposed, const float *src, int64_t rows, int64_t K, int64_t Kp,
+                        int64_t ld, int64_t src_stride, int64_t batch, __nv_bfloat16 *const out[3],
+                        cudaStream_t stream) {
+    SplitArgs a;
+    a.src = src;
+    a.rows = rows;
+    a.K = K;
+    a.Kp = Kp;
+    a.ld = ld;
+    a.src_stride = src_stride;
+    for (int i = 0; i < 3; ++i) a.out[i] = out[i];
+    a.piece_stride = rows * Kp;
+    if (!transposed) {
+        const int64_t total = rows * (Kp / 4);
+        int64_t grid = (total + 255) / 256;
+        const int64_t cap = (int64_t)sm_count() * 16;
+        if (grid > cap) grid = cap;
+        dim3 gr((unsigned)(grid > 0 ? grid : 1), (unsigned)batch);
+        if (np == 1) split_direct_kernel<1><<<gr, 256, 0, stream>>>(a);
+        else if (np == 2) split_direct_kernel<2><<<gr, 256, 0, stream>>>(a);
+        else split_direct_kernel<3><<<gr, 256, 0, stream>>>(a);
+    } else {
+        const int64_t gx = (rows + 31) / 32, gy = (Kp + 31) / 32;
+        if (gy > 65535) return set_error(GATLAS_ERR_INVALID, "matmul: K too large for the transposing split");
+        dim3 gr((unsigned)gx, (unsigned)gy, (unsigned)batch);
+        if (np == 1) split_transpose_kernel<1><<<gr, 256, 0, stream>>>(a);
+        else if (np == 2) split_transpose_kernel<2><<<gr, 256, 0, stream>>>(a);
+        else split_transpose_kernel<3><<<gr, 256, 0, stream>>>(a);
+    }
+    return check_launch("split kernel");
+}
+
+template <int MODE>
+static int launch_tc(const Geometry &g, const Plan &pl, __nv_bfloat16 *const ap[3], __nv_bfloat16 *const bp[3],
+                     float *C, double alpha, double beta, int gemm, cudaStream_t stream) {
+    CUtensorMap ta[3], tb[3];
+    const uint64_t adims[3] = {(uint64_t)pl.Kp, (uint64_t)g.M, (uint64_t)g.batch};
+    const uint64_t astr[2] = {(uint64_t)pl.Kp * 2, (uint64_t)pl.Kp * 2 * (uint64_t)g.M};
+    const uint64_t bdims[3] = {(uint64_t)pl.Kp, (uint64_t)g.N, (uint64_t)g.batch};
+    const uint64_t bstr[2] = {(uint64_t)pl.Kp * 2, (uint64_t)pl.Kp * 2 * (uint64_t)g.N};
+    const uint32_t abox[3] = {BK, BM, 1}, bbox[3] = {BK, BN, 1};
+    for (int i = 0; i < 3; ++i) {
+        const int src = i < pl.np ? i : 0;  // unused slots alias piece 0
+        int rc = make_tensor_map(&ta[i], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, ap[src], adims, astr, abox,
+                                 CU_TENSOR_MAP_SWIZZLE_64B);
+        if (rc) return rc;
+        rc = make_tensor_map(&tb[i], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, bp[src], bdims, bstr, bbox,
+                             CU_TENSOR_MAP_SWIZZLE_64B);
+        if (rc) return rc;
+    }
+    Params p;
+    p.C = C;
+    p.M = g.M;
+    p.N = g.N;
+    p.ldc = g.ldc;
+    p.stride_c = g.stride_c;
+    p.kblocks = (int)((pl.Kp + BK - 1) / BK);
+    p.alpha = (float)alpha;
+    p.beta = (float)beta;
+    p.gemm = gemm;
+    p.fault = device_fault_word();
+    const int smem = (int)Layout<MODE>::SMEM_BYTES;
+    cudaError_t e = cudaFuncSetAttribute(tc_gemm_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "tc gemm smem attribute: %s", cudaGetErrorString(e));
+    const int64_t gx = (g.N + BN - 1) / BN, gy = (g.M + BM - 1) / BM;
+    if (gy > 65535) return set_error(GATLAS_ERR_INVALID, "matmul: M too large for the tensor-core grid");
+    dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)g.batch);
+    tc_gemm_kernel<MODE><<<grid, kThreads, smem, stream>>>(ta[0], ta[1], ta[2], tb[0], tb[1], tb[2], p);
+    return check_launch("tc_gemm_kernel");
+}
+
+}  // namespace tcg
+
+size_t tc_workspace_bytes(const gatlas_matmul_desc *d, const Geometry &g) {
+    tcg::Plan pl;
+    if (!tcg::make_plan(d, g, &pl)) return 0;
+    return pl.total;
+}
+
+int tc_supported(const gatlas_matmul_desc *d) {
+    return d->engine == GATLAS_ENGINE_TC_BF16 || d->engine == GATLAS_ENGINE_TC_SPLIT3 ||
+           d->engine == GATLAS_ENGINE_TC_SPLIT6;
+}
+
+int matmul_tc(const gatlas_matmul_desc *d, const Geometry &g, const float *A, const float *B, float *C, void *ws,
+              size_t ws_bytes, cudaStream_t stream) {
+    using namespace tcg;
+    Plan pl;
+    if (!make_plan(d, g, &pl))
+        return set_error(GATLAS_ERR_UNSUPPORTED, "matmul: tensor-core engine %d not built", d->engine);
+    if (g.K == 0) {
+        // empty contraction: C = beta*C (gemm) or 0; handled by the SIMT path
+        gatlas_matmul_desc s = *d;
+        s.engine = GATLAS_ENGINE_BUFFER;
+        s.group_h = s.group_w = s.block_h = s.block_w = s.vector_length = 0;
+        return gatlas_matmul_f32(&s, A, B, C, nullptr, 0, stream);
+    }
+    if (!ws) {
+        ws = device_scratch(pl.total);
+        if (!ws) return set_error(GATLAS_ERR_NOMEM, "matmul: scratch of %zu bytes", pl.total);
+    } else if (ws_bytes < pl.total) {
+        return set_error(GATLAS_ERR_INVALID, "matmul: workspace %zu < %zu bytes", ws_bytes, pl.total);
+    } else if (!aligned_to(ws, 1024)) {
+        return set_error(GATLAS_ERR_INVALID, "matmul: workspace must be 1024-byte aligned");
+    }
+    uint8_t *base = static_cast<uint8_t *>(ws);
+    __nv_bfloat16 *ap[3] = {nullptr, nullptr, nullptr}, *bp[3] = {nullptr, nullptr, nullptr};
+    for (int i = 0; i < pl.np; ++i) {
+        ap[i] = reinterpret_cast<__nv_bfloat16 *>(base + i * pl.a_piece_bytes);
+        bp[i] = reinterpret_cast<__nv_bfloat16 *>(base + pl.np * pl.a_piece_bytes + i * pl.b_piece_bytes);
+    }
+    // A: K-major already when not transposed; B: K-major when transposed.
+    int rc = launch_split(pl.np, g.ta, A, g.M, g.K, pl.Kp, g.lda, g.stride_a, g.batch, ap, stream);
+    if (rc) return rc;
+    rc = launch_split(pl.np, !g.tb, B, g.N, g.K, pl.Kp, g.ldb, g.stride_b, g.batch, bp, stream);
+    if (rc) return rc;
+    switch (pl.mode) {
+        case 0: return launch_tc<0>(g, pl, ap, bp, C, d->alpha, d->beta, d->gemm, stream);
+        case 1: return launch_tc<1>(g, pl, ap, bp, C, d->alpha, d->beta, d->gemm, stream);
+        default: return launch_tc<2>(g, pl, ap, bp, C, d->alpha, d->beta, d->gemm, stream);
+    }
+}
 
 }  // namespace gatlas

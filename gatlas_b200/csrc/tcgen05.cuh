@@ -1,0 +1,124 @@
+// tcgen05 (5th-generation tensor core) and TMEM helpers for sm_100a, written
+// as inline PTX.  Descriptor bit layouts follow the PTX ISA for tcgen05:
+//   shared-memory matrix descriptor (64 bit): start address >> 4 [0,14),
+//   leading-dimension byte offset >> 4 [16,30), stride-dimension byte offset
+//   >> 4 [32,46), descriptor version 1 [46,48), base offset [49,52), layout
+//   (swizzle) type [61,64) with 0 = none, 2 = 128B, 4 = 64B, 6 = 32B;
+//   instruction descriptor for kind::f16 (32 bit): D format [4,6) (1 = F32),
+//   A format [7,10) and B format [10,13) (0 = F16, 1 = BF16), A/B major
+//   [15], [16] (0 = K-major), N >> 3 [17,23), M >> 4 [24,29).
+#pragma once
+
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace gatlas {
+namespace tc {
+
+#ifdef __CUDACC__
+
+__device__ __forceinline__ uint64_t globaltimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// mbarrier wait bounded in wall time (ns).  Returns false on timeout or when
+// *abort becomes non-zero.
+__device__ __forceinline__ bool wait_timed(uint64_t *bar, uint32_t parity, uint64_t limit_ns,
+                                           volatile int *abort) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer();
+    while (true) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (abort && *abort) return false;
+        if (globaltimer() - t0 > limit_ns) return false;
+    }
+}
+
+enum Swizzle : uint32_t { kSwizzleNone = 0, kSwizzle128B = 2, kSwizzle64B = 4, kSwizzle32B = 6 };
+
+// K-major operand descriptor: 8-row core-matrix groups `sbo_bytes` apart,
+// rows of the swizzle width; the leading byte offset is unused for swizzled
+// K-major layouts and set to 16 bytes.
+__device__ __forceinline__ uint64_t smem_desc_kmajor(uint32_t smem_addr, uint32_t sbo_bytes, uint32_t swz) {
+    uint64_t d = 0;
+    d |= (uint64_t)((smem_addr >> 4) & 0x3FFF);
+    d |= (uint64_t)(1u) << 16;                            // LBO = 16 B (unused)
+    d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFF) << 32;     // SBO
+    d |= (uint64_t)1 << 46;                               // version
+    d |= (uint64_t)(swz & 7u) << 61;                      // layout type
+    return d;
+}
+
+__host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
+    return (1u << 4)                    // D = F32
+           | (1u << 7)                  // A = BF16
+           | (1u << 10)                 // B = BF16
+           | ((uint32_t)(N >> 3) << 17) // N
+           | ((uint32_t)(M >> 4) << 24);// M
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t *smem_dst, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(smem_dst)),
+                 "r"(ncols)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_relinquish() {
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+__device__ __forceinline__ void fence_before_sync() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_after_sync() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// D[tmem] (+)= A[smem desc] * B[smem desc]^T, single CTA, kind::f16.
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// Arrives once on the mbarrier when all previously issued tcgen05 async
+// operations of this thread have completed.
+__device__ __forceinline__ void commit_to(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+// 32 lanes x 32 consecutive 32-bit columns: thread i of the warp receives
+// lane (base lane + i), columns [col, col + 32).
+__device__ __forceinline__ void tmem_ld_32x32b_x32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+          "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+          "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+          "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+#endif  // __CUDACC__
+
+}  // namespace tc
+}  // namespace gatlas

@@ -1,0 +1,94 @@
+"""Tensor-core engines (tcgen05): BF16 in / FP32 out, and FP32 operands split
+into BF16 pieces (3 or 6 products).  Checked against the FP64 oracle: exact on
+the reference's test pattern (C == K), within each engine's error budget on
+uniform[-1,1) inputs, and within 4*K*u when every product is exact (sign*2^e
+inputs, where the BF16 pieces represent the operands exactly)."""
+import numpy as np
+import pytest
+
+import gatlas_b200 as g
+import oracle
+
+pytestmark = pytest.mark.gpu
+U32 = 2.0 ** -24
+ENGINES = ["tc_bf16", "tc_split3", "tc_split6"]
+# normwise error budgets vs FP64 on uniform[-1,1) operands, K <= 1024
+BUDGET = {"tc_bf16": 4e-3, "tc_split3": 2e-5, "tc_split6": 1e-5}
+
+
+def _gpu(cuda, a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to(cuda)
+
+
+def _mm(cuda, A, B, M, N, K, engine, ta=0, tb=0, gemm=False, Cin=None, alpha=1.0, beta=0.0, batch=1):
+    import torch
+    C = _gpu(cuda, Cin) if Cin is not None else torch.full((batch * M * N,), float("nan"), device=cuda)
+    g.matmul(_gpu(cuda, A), _gpu(cuda, B), M, N, K, C=C, trans_a=ta, trans_b=tb, gemm=gemm,
+             alpha=alpha, beta=beta, engine=engine, batch=batch)
+    torch.cuda.synchronize()
+    assert g.device_faults() == 0
+    return C.cpu().numpy()
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_known_answer_c_equals_k(cuda, engine):
+    M = N = K = 1024
+    C = _mm(cuda, np.ones(M * K, np.float32), np.ones(K * N, np.float32), M, N, K, engine)
+    assert oracle.check_pattern(C, float(K))
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("M,N,K", [(128, 256, 32), (200, 300, 100), (257, 129, 520), (64, 1000, 8),
+                                   (1, 1, 1), (512, 512, 1024)])
+def test_uniform_within_budget(cuda, engine, ta, tb, M, N, K):
+    A = oracle.uniform(M * K, seed=M + 3 * K)
+    B = oracle.uniform(K * N, seed=N + 5 * K)
+    C = _mm(cuda, A, B, M, N, K, engine, ta, tb)
+    ref = oracle.matmul(A, B, M, N, K, ta, tb, mode=oracle.F64)
+    assert oracle.normwise_error(C, ref) <= BUDGET[engine]
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_exact_products_meet_fp32_tolerance(cuda, engine):
+    M, N, K = 256, 512, 512
+    A = oracle.pow2(M * K, seed=1)
+    B = oracle.pow2(K * N, seed=2)
+    C = _mm(cuda, A, B, M, N, K, engine)
+    ref = oracle.matmul(A, B, M, N, K, mode=oracle.F64)
+    assert oracle.normwise_error(C, ref) <= 4 * K * U32
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_gemm_alpha_beta_batch(cuda, engine):
+    M, N, K, P = 160, 272, 96, 3
+    A = oracle.uniform(P * M * K, seed=7)
+    B = oracle.uniform(P * K * N, seed=8)
+    Cin = oracle.uniform(P * M * N, seed=9)
+    C = _mm(cuda, A, B, M, N, K, engine, gemm=True, Cin=Cin, alpha=0.5, beta=-2.0, batch=P)
+    ref = oracle.matmul(A, B, M, N, K, mode=oracle.F64, gemm=1, Cin=Cin, alpha=0.5, beta=-2.0,
+                        packed=P)
+    assert oracle.normwise_error(C, ref) <= BUDGET[engine]
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_caller_workspace(cuda, engine):
+    import torch
+    M, N, K = 256, 256, 256
+    ws = torch.empty(g.matmul_workspace_size(M, N, K, engine) + 1024, dtype=torch.uint8, device=cuda)
+    A = oracle.uniform(M * K, seed=1)
+    B = oracle.uniform(K * N, seed=2)
+    C = g.matmul(_gpu(cuda, A), _gpu(cuda, B), M, N, K, engine=engine, workspace=ws)
+    torch.cuda.synchronize()
+    ref = oracle.matmul(A, B, M, N, K, mode=oracle.F64)
+    assert oracle.normwise_error(C.cpu().numpy(), ref) <= BUDGET[engine]
+    with pytest.raises(g.GatlasError):
+        g.matmul(_gpu(cuda, A), _gpu(cuda, B), M, N, K, engine=engine, workspace=ws[:1024])
+
+
+def test_empty_k(cuda):
+    Cin = oracle.uniform(64 * 64, seed=3)
+    C = _mm(cuda, np.zeros(1, np.float32), np.zeros(1, np.float32), 64, 64, 0, "tc_split3",
+            gemm=True, Cin=Cin, alpha=1.0, beta=0.5)
+    assert np.array_equal(C, (Cin * np.float32(0.5)).astype(np.float32))
