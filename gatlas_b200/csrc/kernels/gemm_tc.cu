@@ -35,8 +35,9 @@ namespace gatlas {
 namespace tcg {
 
 constexpr int BM = 128, BN = 256, BK = 32;
-constexpr int kThreads = 128;
-constexpr uint32_t kTmemCols = 256;
+// Default promotion interval: 4 slices of BK = 32, i.e. K = 128 per
+// TMEM segment (selectable per call through the descriptor's extra field).
+constexpr int kDefaultSegKblocks = 4;
 constexpr uint32_t kRowBytes = BK * 2;        // 64 B rows -> 64-byte swizzle
 constexpr uint32_t kSBO = 8 * kRowBytes;      // 8-row core-matrix groups
 constexpr uint32_t kATile = BM * kRowBytes;   // 8 KiB
@@ -80,13 +81,21 @@ struct Params {
     float *C;
     int64_t M, N, ldc, stride_c;
     int kblocks;
+    int seg_kblocks;  // K slices (of BK) accumulated in TMEM before promotion
     float alpha, beta;
     int gemm;
     int *fault;
 };
 
+// Warp roles: warp 0 = TMA producer (lane 0), warp 1 = MMA issuer (lane 0),
+// warps 2..9 = accumulator drain + epilogue.  Drain warp w reads TMEM lane
+// quarter (w % 4) and column half (w - 2) / 4.
+constexpr int kDrainWarps = 8;
+constexpr int kThreads2 = 32 * (2 + kDrainWarps);
+constexpr uint32_t kTmemCols2 = 2 * BN;  // two accumulator buffers
+
 template <int MODE>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads2, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap ta0, const __grid_constant__ CUtensorMap ta1,
                    const __grid_constant__ CUtensorMap ta2, const __grid_constant__ CUtensorMap tb0,
                    const __grid_constant__ CUtensorMap tb1, const __grid_constant__ CUtensorMap tb2,
@@ -96,7 +105,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     constexpr int S = L::STAGES;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    __shared__ __align__(8) uint64_t full[S], empty[S], accf;
+    __shared__ __align__(8) uint64_t full[S], empty[S], tfull[2], tempty[2];
     __shared__ uint32_t tmem_base;
     __shared__ volatile int abort_flag;
     __shared__ int kb_issued, kb_consumed;
@@ -105,13 +114,17 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN, z = blockIdx.z;
     const CUtensorMap *tA[3] = {&ta0, &ta1, &ta2};
     const CUtensorMap *tB[3] = {&tb0, &tb1, &tb2};
+    const int nseg = (p.kblocks + p.seg_kblocks - 1) / p.seg_kblocks;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(&accf, 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], kDrainWarps);
+        }
         fence_mbarrier_init();
         abort_flag = 0;
         kb_issued = 0;
@@ -122,7 +135,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
     }
     if (warp == 0) {
-        tc::tmem_alloc(&tmem_base, kTmemCols);
+        tc::tmem_alloc(&tmem_base, kTmemCols2);
         tc::tmem_relinquish();
     }
     tc::fence_before_sync();
@@ -134,109 +147,145 @@ __global__ void __launch_bounds__(kThreads, 1)
     auto b_tile = [&](int s, int piece) { return smem + s * L::STAGE_BYTES + MD::NP * kATile + piece * kBTile; };
 
     if (warp == 0) {
-      if (lane == 0) {
-        // ---- TMA producer ----
-        int kb = 0;
-        for (; kb < p.kblocks; ++kb) {
-            const int s = kb % S;
-            const uint32_t ph = (uint32_t)(kb / S) & 1u;
-            if (!tc::wait_timed(&empty[s], ph ^ 1u, kWaitNs, &abort_flag)) {
-                if (!abort_flag) report_fault(p.fault, kFaultTcProducerWait);
-                abort_flag = 1;
-                break;
+        if (lane == 0) {
+            // ---- TMA producer ----
+            int kb = 0;
+            for (; kb < p.kblocks; ++kb) {
+                const int s = kb % S;
+                const uint32_t ph = (uint32_t)(kb / S) & 1u;
+                if (!tc::wait_timed(&empty[s], ph ^ 1u, kWaitNs, &abort_flag)) {
+                    if (!abort_flag) report_fault(p.fault, kFaultTcProducerWait);
+                    abort_flag = 1;
+                    break;
+                }
+                mbar_arrive_expect_tx(&full[s], L::STAGE_BYTES);
+                for (int i = 0; i < MD::NP; ++i) {
+                    tma_load_3d(a_tile(s, i), tA[i], kb * BK, m0, z, &full[s]);
+                    tma_load_3d(b_tile(s, i), tB[i], kb * BK, n0, z, &full[s]);
+                }
             }
-            mbar_arrive_expect_tx(&full[s], L::STAGE_BYTES);
-            for (int i = 0; i < MD::NP; ++i) {
-                tma_load_3d(a_tile(s, i), tA[i], kb * BK, m0, z, &full[s]);
-                tma_load_3d(b_tile(s, i), tB[i], kb * BK, n0, z, &full[s]);
+            kb_issued = kb;
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---- MMA issuer: segment g accumulates into TMEM buffer g & 1 ----
+            constexpr uint32_t idesc = tc::idesc_bf16_f32(BM, BN);
+            int kb = 0;
+            for (; kb < p.kblocks; ++kb) {
+                const int seg = kb / p.seg_kblocks, b = seg & 1;
+                const bool seg_first = (kb % p.seg_kblocks) == 0;
+                const bool seg_last = (kb % p.seg_kblocks) == p.seg_kblocks - 1 || kb == p.kblocks - 1;
+                if (seg_first) {
+                    // the drain of this buffer's previous segment must be done
+                    if (!tc::wait_timed(&tempty[b], ((uint32_t)(seg >> 1) & 1u) ^ 1u, kWaitNs, &abort_flag)) {
+                        if (!abort_flag) report_fault(p.fault, kFaultTcMmaWait);
+                        abort_flag = 1;
+                        break;
+                    }
+                    tc::fence_after_sync();
+                }
+                const int s = kb % S;
+                const uint32_t ph = (uint32_t)(kb / S) & 1u;
+                if (!tc::wait_timed(&full[s], ph, kWaitNs, &abort_flag)) {
+                    if (!abort_flag) report_fault(p.fault, kFaultTcMmaWait);
+                    abort_flag = 1;
+                    break;
+                }
+                tc::fence_after_sync();
+                const uint32_t d = tmem + (uint32_t)(b * BN);
+#pragma unroll
+                for (int kk = 0; kk < BK / 16; ++kk) {
+#pragma unroll
+                    for (int j = 0; j < MD::NPROD; ++j) {
+                        const uint32_t a_addr = smem_u32(a_tile(s, MD::pa(j))) + kk * 32;
+                        const uint32_t b_addr = smem_u32(b_tile(s, MD::pb(j))) + kk * 32;
+                        tc::mma_bf16(d, tc::smem_desc_kmajor(a_addr, kSBO, tc::kSwizzle64B),
+                                     tc::smem_desc_kmajor(b_addr, kSBO, tc::kSwizzle64B), idesc,
+                                     (seg_first && kk == 0 && j == 0) ? 0u : 1u);
+                    }
+                }
+                tc::commit_to(&empty[s]);
+                if (seg_last) tc::commit_to(&tfull[b]);
+            }
+            kb_consumed = kb;
+            if (kb < p.kblocks) {
+                // aborted: make sure every issued MMA has completed before TMEM is freed
+                tc::commit_to(&tfull[0]);
             }
         }
-        kb_issued = kb;
-      }
-      __syncwarp();
-    } else if (warp == 1) {
-      if (lane == 0) {
-        // ---- MMA issuer ----
-        constexpr uint32_t idesc = tc::idesc_bf16_f32(BM, BN);
-        int kb = 0;
-        for (; kb < p.kblocks; ++kb) {
-            const int s = kb % S;
-            const uint32_t ph = (uint32_t)(kb / S) & 1u;
-            if (!tc::wait_timed(&full[s], ph, kWaitNs, &abort_flag)) {
-                if (!abort_flag) report_fault(p.fault, kFaultTcMmaWait);
+        __syncwarp();
+    } else {
+        // ---- drain: promote each segment into round-to-nearest FP32 sums ----
+        const int quarter = warp & 3, half = (warp - 2) >> 2;
+        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+        float acc[BN / 2];
+#pragma unroll
+        for (int j = 0; j < BN / 2; ++j) acc[j] = 0.0f;
+        bool ok = true;
+        for (int seg = 0; seg < nseg; ++seg) {
+            const int b = seg & 1;
+            if (!tc::wait_timed(&tfull[b], (uint32_t)(seg >> 1) & 1u, 2 * kWaitNs, &abort_flag)) {
+                if (!abort_flag) report_fault(p.fault, kFaultTcEpilogueWait);
                 abort_flag = 1;
+                ok = false;
                 break;
             }
             tc::fence_after_sync();
 #pragma unroll
-            for (int kk = 0; kk < BK / 16; ++kk) {
+            for (int c = 0; c < BN / 2 / 32; ++c) {
+                uint32_t r[32];
+                tc::tmem_ld_32x32b_x32(tmem + lane_base + (uint32_t)(b * BN + half * (BN / 2) + c * 32), r);
+                tc::tmem_ld_wait();
 #pragma unroll
-                for (int j = 0; j < MD::NPROD; ++j) {
-                    const uint32_t a_addr = smem_u32(a_tile(s, MD::pa(j))) + kk * 32;
-                    const uint32_t b_addr = smem_u32(b_tile(s, MD::pb(j))) + kk * 32;
-                    tc::mma_bf16(tmem, tc::smem_desc_kmajor(a_addr, kSBO, tc::kSwizzle64B),
-                                 tc::smem_desc_kmajor(b_addr, kSBO, tc::kSwizzle64B), idesc,
-                                 (kb | kk | j) != 0 ? 1u : 0u);
-                }
+                for (int j = 0; j < 32; ++j) acc[c * 32 + j] = __fadd_rn(acc[c * 32 + j], __uint_as_float(r[j]));
             }
-            tc::commit_to(&empty[s]);
+            tc::fence_before_sync();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[b]);
         }
-        kb_consumed = kb;
-        tc::commit_to(&accf);  // fires when every MMA issued above has completed
-      }
-      __syncwarp();
-    }
-
-    // ---- epilogue: TMEM -> registers -> C ----
-    const bool acc_ready = tc::wait_timed(&accf, 0, 2 * kWaitNs, nullptr);
-    if (!acc_ready && threadIdx.x == 0) report_fault(p.fault, kFaultTcEpilogueWait);
-    tc::fence_after_sync();
-    __syncthreads();
-    if (acc_ready && !abort_flag) {
-        const int64_t row = (int64_t)m0 + warp * 32 + lane;
-        float *crow = p.C + (int64_t)z * p.stride_c + row * p.ldc;
-        const bool vec_ok = (p.ldc % 4 == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0) &&
-                            (p.stride_c % 4 == 0);
-#pragma unroll 1
-        for (int c = 0; c < BN / 32; ++c) {
-            uint32_t r[32];
-            tc::tmem_ld_32x32b_x32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * 32), r);
-            tc::tmem_ld_wait();
+        if (ok && !abort_flag) {
+            const int64_t row = (int64_t)m0 + quarter * 32 + lane;
+            float *crow = p.C + (int64_t)z * p.stride_c + row * p.ldc;
+            const bool vec_ok = (p.ldc % 4 == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0) &&
+                                (p.stride_c % 4 == 0);
             if (row < p.M) {
-                const int64_t col0 = (int64_t)n0 + c * 32;
-                float v[32];
+                const int64_t col0 = (int64_t)n0 + half * (BN / 2);
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const float acc = __uint_as_float(r[j]);
-                    if (p.gemm) {
-                        const int64_t col = col0 + j;
-                        const float bc = (p.beta == 0.0f || col >= p.N) ? 0.0f : p.beta * crow[col];
-                        v[j] = __fmaf_rn(p.alpha, acc, bc);
-                    } else {
-                        v[j] = acc;
+                for (int j = 0; j < BN / 2; j += 4) {
+                    float v[4];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const int64_t col = col0 + j + e;
+                        if (p.gemm) {
+                            const float bc = (p.beta == 0.0f || col >= p.N) ? 0.0f : p.beta * crow[col];
+                            v[e] = __fmaf_rn(p.alpha, acc[j + e], bc);
+                        } else {
+                            v[e] = acc[j + e];
+                        }
                     }
-                }
-                if (vec_ok && col0 + 31 < p.N) {
+                    if (vec_ok && col0 + j + 3 < p.N) {
+                        *reinterpret_cast<float4 *>(crow + col0 + j) = make_float4(v[0], v[1], v[2], v[3]);
+                    } else {
 #pragma unroll
-                    for (int j = 0; j < 32; j += 4)
-                        *reinterpret_cast<float4 *>(crow + col0 + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
-                } else {
-#pragma unroll
-                    for (int j = 0; j < 32; ++j)
-                        if (col0 + j < p.N) crow[col0 + j] = v[j];
+                        for (int e = 0; e < 4; ++e)
+                            if (col0 + j + e < p.N) crow[col0 + j + e] = v[e];
+                    }
                 }
             }
         }
     }
     tc::fence_before_sync();
     __syncthreads();
-    // after an abort: wait (bounded) for copies still landing in shared memory
     if (threadIdx.x == 0 && abort_flag) {
+        // wait (bounded) for copies still landing in shared memory and for
+        // the MMAs issued before the abort
         for (int kb = kb_consumed; kb < kb_issued; ++kb)
             tc::wait_timed(&full[kb % S], (uint32_t)(kb / S) & 1u, kWaitNs, nullptr);
+        if (kb_consumed < p.kblocks) tc::wait_timed(&tfull[0], 0, kWaitNs, nullptr);
     }
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, kTmemCols);
+    if (warp == 0) tc::tmem_dealloc(tmem, kTmemCols2);
 }
 
 // ---------------------------------------------------------------------------
@@ -377,7 +426,7 @@ static int launch_split(int np, bool transposed, const float *src, int64_t rows,
 
 template <int MODE>
 static int launch_tc(const Geometry &g, const Plan &pl, __nv_bfloat16 *const ap[3], __nv_bfloat16 *const bp[3],
-                     float *C, double alpha, double beta, int gemm, cudaStream_t stream) {
+                     float *C, double alpha, double beta, int gemm, int seg_kblocks, cudaStream_t stream) {
     CUtensorMap ta[3], tb[3];
     const uint64_t adims[3] = {(uint64_t)pl.Kp, (uint64_t)g.M, (uint64_t)g.batch};
     const uint64_t astr[2] = {(uint64_t)pl.Kp * 2, (uint64_t)pl.Kp * 2 * (uint64_t)g.M};
@@ -400,6 +449,7 @@ static int launch_tc(const Geometry &g, const Plan &pl, __nv_bfloat16 *const ap[
     p.ldc = g.ldc;
     p.stride_c = g.stride_c;
     p.kblocks = (int)((pl.Kp + BK - 1) / BK);
+    p.seg_kblocks = seg_kblocks > 0 ? seg_kblocks : kDefaultSegKblocks;
     p.alpha = (float)alpha;
     p.beta = (float)beta;
     p.gemm = gemm;
@@ -410,7 +460,7 @@ static int launch_tc(const Geometry &g, const Plan &pl, __nv_bfloat16 *const ap[
     const int64_t gx = (g.N + BN - 1) / BN, gy = (g.M + BM - 1) / BM;
     if (gy > 65535) return set_error(GATLAS_ERR_INVALID, "matmul: M too large for the tensor-core grid");
     dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)g.batch);
-    tc_gemm_kernel<MODE><<<grid, kThreads, smem, stream>>>(ta[0], ta[1], ta[2], tb[0], tb[1], tb[2], p);
+    tc_gemm_kernel<MODE><<<grid, kThreads2, smem, stream>>>(ta[0], ta[1], ta[2], tb[0], tb[1], tb[2], p);
     return check_launch("tc_gemm_kernel");
 }
 
@@ -460,9 +510,9 @@ int matmul_tc(const gatlas_matmul_desc *d, const Geometry &g, const float *A, co
     rc = launch_split(pl.np, !g.tb, B, g.N, g.K, pl.Kp, g.ldb, g.stride_b, g.batch, bp, stream);
     if (rc) return rc;
     switch (pl.mode) {
-        case 0: return launch_tc<0>(g, pl, ap, bp, C, d->alpha, d->beta, d->gemm, stream);
-        case 1: return launch_tc<1>(g, pl, ap, bp, C, d->alpha, d->beta, d->gemm, stream);
-        default: return launch_tc<2>(g, pl, ap, bp, C, d->alpha, d->beta, d->gemm, stream);
+        case 0: return launch_tc<0>(g, pl, ap, bp, C, d->alpha, d->beta, d->gemm, (int)d->extra, stream);
+        case 1: return launch_tc<1>(g, pl, ap, bp, C, d->alpha, d->beta, d->gemm, (int)d->extra, stream);
+        default: return launch_tc<2>(g, pl, ap, bp, C, d->alpha, d->beta, d->gemm, (int)d->extra, stream);
     }
 }
 

@@ -109,7 +109,10 @@ int gatlas_matvec_f64(const gatlas_matvec_desc *d, const double *A, const double
  * Replaces KernelMatmulBuffer<SCALAR,VL> and KernelMatmulImage<SCALAR,VL>
  * (KernelMatmulBuffer.hpp:174-342, KernelMatmulImage.hpp:192-313).
  * SIMT engines accumulate k = 0..K-1 as one fused multiply-add chain per
- * element, bit-exact against a sequential fmaf chain. */
+ * element, bit-exact against a sequential fmaf chain.  For the TC_* engines
+ * the tile fields are ignored and `extra` is the promotion interval: the
+ * tensor cores accumulate `extra` slices of K = 32 in TMEM before the partial
+ * sum is added into round-to-nearest FP32 registers (0 selects 4, K = 128). */
 typedef struct gatlas_matmul_desc {
     int32_t engine;
     int32_t gemm;
