@@ -13,7 +13,8 @@ pytestmark = pytest.mark.gpu
 U32 = 2.0 ** -24
 ENGINES = ["tc_bf16", "tc_split3", "tc_split6"]
 # normwise error budgets vs FP64 on uniform[-1,1) operands, K <= 1024
-BUDGET = {"tc_bf16": 4e-3, "tc_split3": 8e-6, "tc_split6": 2.5e-6}
+# BF16 rounds each operand with unit roundoff 2^-8, so one product can be off by 2^-7
+BUDGET = {"tc_bf16": 2.0 ** -7, "tc_split3": 8e-6, "tc_split6": 2.5e-6}
 
 
 def _gpu(cuda, a):
