@@ -381,3 +381,69 @@ extern "C" int gatlas_matvec_f64(const gatlas_matvec_desc *d, const double *A, c
                                  double *y, void *workspace, size_t workspace_bytes, void *stream) {
     return gatlas::matvec_launch<double>(d, A, x, y, workspace, workspace_bytes, (cudaStream_t)stream);
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free GEMV entry point.
+//
+// For callers that cannot call cudaMalloc: code that runs inside a host
+// framework which owns all device memory (or has reserved it for its own
+// pool), and code on a latency-critical path that must not trigger the
+// device-wide synchronisation cudaMalloc/cudaFree imply.  The column-major
+// path needs scratch for per-segment partial sums and arrival counters; this
+// entry point takes it from a fixed 1 MiB array in device memory that this
+// file owns, instead of from a workspace or the library's allocation cache.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace gatlas {
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = GATLAS_MATVEC_NOALLOC_SCRATCH_BYTES;
+
+// One copy per GPU that loads this library, held until the process exits.
+// Host code may not use this name as a device address: the device address is
+// looked up once per device with cudaGetSymbolAddress.
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
+
+// Device address of g_noalloc_scratch for the current device (looked up on
+// the first call on each device, with that device current).
+int noalloc_scratch(void **out) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "matvec_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return set_error(GATLAS_ERR_INVALID, "matvec_noalloc: device %d", dev);
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return set_error(GATLAS_ERR_CUDA, "matvec_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return GATLAS_OK;
+}
+
+}  // namespace
+}  // namespace gatlas
+
+extern "C" int gatlas_matvec_f32_noalloc(const gatlas_matvec_desc *d, const float *A, const float *x, float *y,
+                                         void *stream) {
+    using namespace gatlas;
+    if (!d) return set_error(GATLAS_ERR_INVALID, "matvec_noalloc: null descriptor");
+    const size_t need = matvec_ws<float>(d, A, x);
+    if (need > kNoAllocScratchBytes)
+        return set_error(GATLAS_ERR_INVALID,
+                         "matvec_noalloc: this problem needs %zu bytes of scratch, more than the %zu-byte "
+                         "static scratch of the allocation-free entry point; call gatlas_matvec_f32 with a "
+                         "workspace instead",
+                         need, kNoAllocScratchBytes);
+    void *scratch = nullptr;
+    const int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    return matvec_launch<float>(d, A, x, y, scratch, kNoAllocScratchBytes, (cudaStream_t)stream);
+}

@@ -94,6 +94,24 @@ int gatlas_matvec_f32(const gatlas_matvec_desc *d, const float *A, const float *
 int gatlas_matvec_f64(const gatlas_matvec_desc *d, const double *A, const double *x, double *y,
                       void *workspace, size_t workspace_bytes, void *stream);
 
+/* Allocation-free float GEMV.  No counterpart in the reference: it exists for
+ * callers that cannot call cudaMalloc -- code inside a host framework that
+ * owns all device memory, and latency-critical code that must not trigger the
+ * device-wide synchronisation of cudaMalloc/cudaFree.  Same arguments and
+ * results as gatlas_matvec_f32 without the workspace: the scratch of the
+ * column-major path (per-segment partial sums and arrival counters) comes
+ * from a fixed GATLAS_MATVEC_NOALLOC_SCRATCH_BYTES array of device memory
+ * inside the library, which every GPU that loads the library holds until the
+ * process exits.  The first call on each device looks the array's device
+ * address up (cudaGetSymbolAddress), so make that first call before any stream
+ * capture.  Problems that need more scratch are rejected with
+ * GATLAS_ERR_INVALID.  All calls share the one array and each call clears
+ * the counters it needs, so calls that overlap on the GPU (concurrent streams,
+ * several host threads) race; serialise them. */
+#define GATLAS_MATVEC_NOALLOC_SCRATCH_BYTES ((size_t)1 << 20)
+int gatlas_matvec_f32_noalloc(const gatlas_matvec_desc *d, const float *A, const float *x, float *y,
+                              void *stream);
+
 /* ---- GEMM ---------------------------------------------------------------
  * C[p] = op(A[p])·op(B[p]) (gemm == 0) or alpha·op(A[p])·op(B[p]) + beta·C[p]
  * (gemm == 1; C is not read when beta == 0).  Layouts follow the reference
