@@ -54,6 +54,10 @@ def _peaks():
                 "source": "fallback"}
 
 
+# DRAM bytes per launch of the split3 contraction at 8192^3 from an ncu capture
+# (None until captured); see profiles/.
+TC_TRAFFIC_BYTES = None
+
 # nominal FP32 SIMT peak: 148 SMs x 128 FP32 lanes x 2 flop x 1.965 GHz
 FP32_SIMT_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
@@ -151,11 +155,8 @@ def _max_over_ranks(x: float, world: int) -> float:
 # our implementation
 # ---------------------------------------------------------------------------
 
-def _fp32_engine(g):
-    for eng in ("tc_split3",):
-        if g.matmul_supported(eng):
-            return eng
-    return "buffer"
+HEADLINE_ENGINE = "tc_split3"     # FP32 operands as BF16 hi/lo, 3 products, FP32 accumulation
+PRODUCTS = {"tc_bf16": 1, "tc_split3": 3, "tc_split6": 6}
 
 
 def _timed(fn, steps, warmup, world, stream):
@@ -176,6 +177,12 @@ def _timed(fn, steps, warmup, world, stream):
     return start.elapsed_time(stop) / steps  # ms per step
 
 
+def _gemm_step_fn(g, A, B, C, M, N, K, engine, ws):
+    def step():
+        g.matmul(A, B, M, N, K, C=C, engine=engine, workspace=ws)
+    return step
+
+
 def run_ours(args, rank, world, local):
     import torch
 
@@ -185,26 +192,20 @@ def run_ours(args, rank, world, local):
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
     peaks = _peaks()
-    engine = _fp32_engine(g)
+    engine = HEADLINE_ENGINE if g.matmul_supported(HEADLINE_ENGINE) else "buffer"
 
-    # ---- headline: SGEMM 8192^3 --------------------------------------------
+    # ---- headline: FP32-accurate SGEMM 8192^3 --------------------------------
     M = N = K = M_GEMM
     A = torch.empty(M * K, dtype=torch.float32, device=dev)
     B = torch.empty(K * N, dtype=torch.float32, device=dev)
     C = torch.empty(M * N, dtype=torch.float32, device=dev)
     g.fill(A, "uniform", seed=1 + rank)
     g.fill(B, "uniform", seed=2 + rank)
-    ws_bytes = g.matmul_workspace_size(M, N, K, engine)
-    ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
-    launches_per_step = 1 if engine == "buffer" else 3
-
-    def step():
-        g.matmul(A, B, M, N, K, C=C, engine=engine, workspace=ws if ws_bytes else None)
-
-    step()
-    torch.cuda.synchronize()
-    fro, refn, mx, _ = g.residual(A, B, C, M, N, K)
-    err = fro / refn
+    ws_bytes = max(g.matmul_workspace_size(M, N, K, e) for e in PRODUCTS)
+    ws = torch.empty(ws_bytes + 1024, dtype=torch.uint8, device=dev)
+    ws = ws[(-ws.data_ptr()) % 1024:][:ws_bytes]          # 1024-byte aligned view
+    step = _gemm_step_fn(g, A, B, C, M, N, K, engine, ws if engine != "buffer" else None)
+    launches_per_step = 1 if engine == "buffer" else 3     # split A, split B, contraction
 
     sampler = ClockSampler(local)
     sampler.start()
@@ -213,47 +214,71 @@ def run_ours(args, rank, world, local):
     ms_max = _max_over_ranks(ms, world)
     flops = 2.0 * M * N * K
     value = world * flops / (ms_max * 1e-3) / 1e12
+    fro, refn, mx, _ = g.residual(A, B, C, M, N, K)
 
-    # kernel-only time of the dominant kernel (the GEMM launch itself)
-    if engine == "buffer":
-        dom_ms = ms
-        roofline = {"bound": "fp32_simt", "achieved": flops / (dom_ms * 1e-3) / 1e12,
-                    "peak": FP32_SIMT_NOMINAL_TFLOPS, "unit": "TFLOP/s",
-                    "peak_source": "nominal (148 SMs x 128 FP32 lanes x 2 x 1.965 GHz); "
-                                   "no measured FP32 SIMT peak on this pool",
-                    "traffic": None}
-        roofline["frac"] = roofline["achieved"] / roofline["peak"]
+    # dominant kernel alone: the tcgen05 contraction on prepared operands
+    if engine != "buffer":
+        g.matmul_tc_prepare(A, B, M, N, K, ws, engine=engine)
+        run_ms = _timed(lambda: g.matmul_tc_run(ws, M, N, K, C, engine=engine), args.steps, 2,
+                        world, stream)
+        ach = PRODUCTS[engine] * flops / (run_ms * 1e-3) / 1e12
+        roofline = {"bound": "tensor", "kernel": "tc_gemm_kernel<split3>", "achieved": ach,
+                    "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
+                    "frac": ach / peaks["bf16_tflops"], "traffic": TC_TRAFFIC_BYTES,
+                    "kernel_ms": run_ms, "kernel_fp32_equiv_tflops": flops / (run_ms * 1e-3) / 1e12,
+                    "peak_source": f"{peaks['source']} dense BF16 (burst, cuBLAS); achieved counts all "
+                                   f"{PRODUCTS[engine]} BF16 products per FP32 multiply-add; 'of measured'",
+                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
+                                      "profiles/tc_gemm_kernel_split3_8192.md"}
     else:
-        dom_ms = ms
-        pk = peaks["bf16_tflops"]
-        ach = 3 * flops / (dom_ms * 1e-3) / 1e12
-        roofline = {"bound": "tensor", "achieved": ach, "peak": pk, "unit": "TFLOP/s",
-                    "frac": ach / pk, "traffic": None,
-                    "peak_source": f"{peaks['source']} bf16 (burst); 3 BF16 products per FP32 MAC"}
+        roofline = {"bound": "fp32_simt", "achieved": value, "peak": FP32_SIMT_NOMINAL_TFLOPS,
+                    "unit": "TFLOP/s", "frac": value / FP32_SIMT_NOMINAL_TFLOPS, "traffic": None,
+                    "peak_source": "nominal (148 SMs x 128 lanes x 2 x 1.965 GHz)"}
 
-    # ---- e2e through the C ABI with host buffers -----------------------------
+    # ---- e2e through the C ABI with host buffers ------------------------------
     hA = torch.empty(M * K, dtype=torch.float32, pin_memory=True)
     hB = torch.empty(K * N, dtype=torch.float32, pin_memory=True)
     hC = torch.empty(M * N, dtype=torch.float32, pin_memory=True)
-    hA.copy_(A, non_blocking=False)
-    hB.copy_(B, non_blocking=False)
+    hA.copy_(A)
+    hB.copy_(B)
 
     def e2e_step():
         A.copy_(hA, non_blocking=True)
         B.copy_(hB, non_blocking=True)
-        g.matmul(A, B, M, N, K, C=C, engine=engine, workspace=ws if ws_bytes else None)
+        step()
         hC.copy_(C, non_blocking=True)
 
-    e2e_steps = max(2, min(args.steps, 10))
-    e2e_ms = _max_over_ranks(_timed(e2e_step, e2e_steps, 1, world, stream), world)
+    e2e_ms = _max_over_ranks(_timed(e2e_step, max(2, min(args.steps, 10)), 1, world, stream), world)
     e2e = {"value": world * flops / (e2e_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
            "h2d_bytes_per_step": 2 * M * K * 4, "d2h_bytes_per_step": M * N * 4,
-           "ms_per_step": e2e_ms}
+           "ms_per_step": e2e_ms, "path": "pinned host A, B -> device, gatlas_matmul_f32, C -> host"}
     del hA, hB, hC
 
-    # ---- secondary: memory-bound pair ----------------------------------------
+    # ---- precision sweep (8192^3; DGEMM 4096^3) -------------------------------
+    sweep = {}
+    if not args.quick:
+        for dist in ("uniform", "pow2"):
+            g.fill(A, dist, seed=11)
+            g.fill(B, dist, seed=12)
+            for eng in ("buffer", "tc_bf16", "tc_split3", "tc_split6"):
+                f = _gemm_step_fn(g, A, B, C, M, N, K, eng, ws if eng != "buffer" else None)
+                t = _timed(f, 3 if eng == "buffer" else 5, 1, world, stream)
+                fr, rn, mxe, _ = g.residual(A, B, C, M, N, K)
+                sweep[f"{eng}_{dist}"] = {"tflops": flops / (t * 1e-3) / 1e12, "ms": t,
+                                          "normwise_err": fr / rn, "max_abs_err": mxe}
+        Md = 4096
+        Ad = torch.empty(Md * Md, dtype=torch.float64, device=dev)
+        Bd = torch.empty(Md * Md, dtype=torch.float64, device=dev)
+        Cd = torch.empty(Md * Md, dtype=torch.float64, device=dev)
+        g.fill(Ad, "uniform", seed=13)
+        g.fill(Bd, "uniform", seed=14)
+        t = _timed(lambda: g.matmul(Ad, Bd, Md, Md, Md, C=Cd), 3, 1, world, stream)
+        sweep["dgemm_buffer_4096"] = {"tflops": 2.0 * Md ** 3 / (t * 1e-3) / 1e12, "ms": t}
+        del Ad, Bd, Cd
+    del C, ws
+
+    # ---- memory-bound pair (config 2) -----------------------------------------
     secondary = {}
-    del C
     Ag = torch.empty(N_GEMV * N_GEMV, dtype=torch.float32, device=dev)
     xg = torch.empty(N_GEMV, dtype=torch.float32, device=dev)
     yg = torch.empty(N_GEMV, dtype=torch.float32, device=dev)
@@ -278,8 +303,9 @@ def run_ours(args, rank, world, local):
         t = _timed(lambda: g.saxpy(0.5, xs, ys, out=ys, engine=eng), max(args.steps, 10), 3,
                    world, stream)
         secondary[f"saxpy_{eng}_gbs"] = 12.0 * N_SAXPY / (t * 1e-3) / 1e9
-    for k in list(secondary):
+    for k in [k for k in secondary if k.endswith("_gbs")]:
         secondary[k.replace("_gbs", "_hbm_frac")] = secondary[k] / peaks["hbm_gbs"]
+    secondary["hbm_peak_gbs"] = peaks["hbm_gbs"]
     del xs, ys
 
     faults = g.device_faults()
@@ -292,10 +318,12 @@ def run_ours(args, rank, world, local):
         "data": "synthetic (seeded uniform[-1,1) FP32 operands generated on the device)",
         "config": {"workload": "sgemm_fp32_accurate_8192", "m": M, "n": N, "k": K,
                    "engine": engine, "layout": "row-major, no transposes",
+                   "step": "split A and B into BF16 pieces + tcgen05 contraction (one "
+                           "gatlas_matmul_f32 call)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "operands larger than L2; no flush"},
-        "error_vs_fp64": {"normwise": err, "max_abs": mx},
-        "e2e": e2e, "roofline": roofline, "secondary": secondary,
+        "error_vs_fp64": {"normwise": fro / refn, "max_abs": mx},
+        "e2e": e2e, "roofline": roofline, "precision_sweep": sweep, "secondary": secondary,
         "gpu_launches": launches_per_step * args.steps, "clocks": clocks,
         "device_faults": faults,
     }
@@ -376,6 +404,55 @@ def run_reference(args, rank, world):
     }
 
 
+def run_case(spec: str) -> None:
+    """Small single-kernel cases for ncu captures: NAME:SIZE, three calls each.
+    tc_bf16|tc_split3|tc_split6:M (M^3 GEMM, prepare once, run x3), sgemm_simt:M,
+    gemv_A:N / gemv_At:N (N^2 GEMV), saxpy_buffer:n / saxpy_image:n."""
+    import torch
+
+    import gatlas_b200 as g
+    name, size = spec.split(":")
+    size = int(size)
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    if name.startswith("tc_") or name == "sgemm_simt":
+        M = size
+        A = torch.empty(M * M, device=dev)
+        B = torch.empty(M * M, device=dev)
+        C = torch.empty(M * M, device=dev)
+        g.fill(A, "uniform", seed=1)
+        g.fill(B, "uniform", seed=2)
+        if name == "sgemm_simt":
+            for _ in range(3):
+                g.matmul(A, B, M, M, M, C=C)
+        else:
+            ws = torch.empty(g.matmul_workspace_size(M, M, M, name) + 1024, dtype=torch.uint8, device=dev)
+            ws = ws[(-ws.data_ptr()) % 1024:]
+            g.matmul_tc_prepare(A, B, M, M, M, ws, engine=name)
+            for _ in range(3):
+                g.matmul_tc_run(ws, M, M, M, C, engine=name)
+    elif name.startswith("gemv_"):
+        N = size
+        A = torch.empty(N * N, device=dev)
+        x = torch.empty(N, device=dev)
+        y = torch.empty(N, device=dev)
+        g.fill(A, "uniform", seed=1)
+        g.fill(x, "uniform", seed=2)
+        for _ in range(3):
+            g.matvec(A, x, N, N, y=y, trans_a=(name == "gemv_At"))
+    elif name.startswith("saxpy_"):
+        x = torch.empty(size, device=dev)
+        y = torch.empty(size, device=dev)
+        g.fill(x, "uniform", seed=1)
+        g.fill(y, "uniform", seed=2)
+        for _ in range(3):
+            g.saxpy(0.5, x, y, out=y, engine=name.split("_")[1])
+    else:
+        raise SystemExit(f"unknown case {spec}")
+    torch.cuda.synchronize()
+    print(json.dumps({"case": spec, "faults": g.device_faults()}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -385,7 +462,12 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="CPU work in the cpu_baseline sample")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--quick", action="store_true", help="skip the precision sweep")
+    ap.add_argument("--case", default=None, help="run one small single-kernel case (for ncu) and exit")
     args = ap.parse_args()
+    if args.case:
+        run_case(args.case)
+        return
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
 

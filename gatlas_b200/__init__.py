@@ -80,6 +80,9 @@ def lib() -> ctypes.CDLL:
     for n in ("gatlas_matmul_f32", "gatlas_matmul_f64"):
         getattr(L, n).argtypes = [ctypes.POINTER(MatmulDesc), vp, vp, vp, vp, sz, vp]
     L.gatlas_matmul_supported.argtypes = [i32, ctypes.POINTER(MatmulDesc)]
+    L.gatlas_matmul_tc_prepare.argtypes = [ctypes.POINTER(MatmulDesc), vp, vp, vp, sz, vp]
+    L.gatlas_matmul_tc_run.argtypes = [ctypes.POINTER(MatmulDesc), vp, sz, vp, vp]
+    L.gatlas_matvec_f32_noalloc.argtypes = [ctypes.POINTER(MatvecDesc), vp, vp, vp, vp]
     L.gatlas_fill_f32.argtypes = [vp, sz, i32, u64, u64, ctypes.c_float, vp]
     L.gatlas_fill_f64.argtypes = [vp, sz, i32, u64, u64, ctypes.c_double, vp]
     L.gatlas_matmul_residual_f32.argtypes = [ctypes.POINTER(MatmulDesc), vp, vp, vp,
@@ -206,6 +209,27 @@ def matmul(A, B, M, N, K, C=None, trans_a=False, trans_b=False, gemm=False, alph
     ws = _ptr(workspace)
     wsb = 0 if workspace is None else workspace.numel() * workspace.element_size()
     check(fn(ctypes.byref(d), _ptr(A), _ptr(B), _ptr(C), ws, wsb, _stream(stream)))
+    return C
+
+
+def matmul_tc_prepare(A, B, M, N, K, workspace, trans_a=False, trans_b=False, engine="tc_split3",
+                      batch=1, extra=0, stream=None):
+    """Writes the BF16 pieces of A and B into `workspace` (tensor-core engines)."""
+    d = matmul_desc(M, N, K, trans_a, trans_b, engine=engine, batch=batch,
+                    tile=(0, 0, 0, 0, 0, extra))
+    check(lib().gatlas_matmul_tc_prepare(ctypes.byref(d), _ptr(A), _ptr(B), _ptr(workspace),
+                                         workspace.numel() * workspace.element_size(),
+                                         _stream(stream)))
+
+
+def matmul_tc_run(workspace, M, N, K, C, trans_a=False, trans_b=False, engine="tc_split3",
+                  gemm=False, alpha=1.0, beta=0.0, batch=1, extra=0, stream=None):
+    """Contracts the pieces prepared in `workspace` into C."""
+    d = matmul_desc(M, N, K, trans_a, trans_b, gemm, alpha, beta, engine, batch=batch,
+                    tile=(0, 0, 0, 0, 0, extra))
+    check(lib().gatlas_matmul_tc_run(ctypes.byref(d), _ptr(workspace),
+                                     workspace.numel() * workspace.element_size(), _ptr(C),
+                                     _stream(stream)))
     return C
 
 

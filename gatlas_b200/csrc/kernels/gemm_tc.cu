@@ -464,6 +464,55 @@ static int launch_tc(const Geometry &g, const Plan &pl, __nv_bfloat16 *const ap[
     return check_launch("tc_gemm_kernel");
 }
 
+// Piece pointers inside a prepared workspace.
+static void piece_ptrs(const Plan &pl, void *ws, __nv_bfloat16 *ap[3], __nv_bfloat16 *bp[3]) {
+    uint8_t *base = static_cast<uint8_t *>(ws);
+    for (int i = 0; i < 3; ++i) {
+        ap[i] = bp[i] = nullptr;
+        if (i < pl.np) {
+            ap[i] = reinterpret_cast<__nv_bfloat16 *>(base + i * pl.a_piece_bytes);
+            bp[i] = reinterpret_cast<__nv_bfloat16 *>(base + pl.np * pl.a_piece_bytes + i * pl.b_piece_bytes);
+        }
+    }
+}
+
+static int check_ws(const Plan &pl, const void *ws, size_t ws_bytes) {
+    if (!ws) return set_error(GATLAS_ERR_INVALID, "matmul: null workspace");
+    if (ws_bytes < pl.total) return set_error(GATLAS_ERR_INVALID, "matmul: workspace %zu < %zu bytes", ws_bytes, pl.total);
+    if (!aligned_to(ws, 1024)) return set_error(GATLAS_ERR_INVALID, "matmul: workspace must be 1024-byte aligned");
+    return GATLAS_OK;
+}
+
+int tc_prepare(const gatlas_matmul_desc *d, const Geometry &g, const float *A, const float *B, void *ws,
+               size_t ws_bytes, cudaStream_t stream) {
+    Plan pl;
+    if (!make_plan(d, g, &pl)) return set_error(GATLAS_ERR_UNSUPPORTED, "matmul: tensor-core engine %d not built", d->engine);
+    int rc = check_ws(pl, ws, ws_bytes);
+    if (rc) return rc;
+    __nv_bfloat16 *ap[3], *bp[3];
+    piece_ptrs(pl, ws, ap, bp);
+    // A is K-major already when not transposed; B is K-major when transposed.
+    rc = launch_split(pl.np, g.ta, A, g.M, g.K, pl.Kp, g.lda, g.stride_a, g.batch, ap, stream);
+    if (rc) return rc;
+    return launch_split(pl.np, !g.tb, B, g.N, g.K, pl.Kp, g.ldb, g.stride_b, g.batch, bp, stream);
+}
+
+int tc_run(const gatlas_matmul_desc *d, const Geometry &g, const void *ws, size_t ws_bytes, float *C,
+           cudaStream_t stream) {
+    Plan pl;
+    if (!make_plan(d, g, &pl)) return set_error(GATLAS_ERR_UNSUPPORTED, "matmul: tensor-core engine %d not built", d->engine);
+    int rc = check_ws(pl, ws, ws_bytes);
+    if (rc) return rc;
+    if (g.K == 0) return set_error(GATLAS_ERR_INVALID, "matmul: K == 0 has no prepared operands");
+    __nv_bfloat16 *ap[3], *bp[3];
+    piece_ptrs(pl, const_cast<void *>(ws), ap, bp);
+    switch (pl.mode) {
+        case 0: return launch_tc<0>(g, pl, ap, bp, C, d->alpha, d->beta, d->gemm, (int)d->extra, stream);
+        case 1: return launch_tc<1>(g, pl, ap, bp, C, d->alpha, d->beta, d->gemm, (int)d->extra, stream);
+        default: return launch_tc<2>(g, pl, ap, bp, C, d->alpha, d->beta, d->gemm, (int)d->extra, stream);
+    }
+}
+
 }  // namespace tcg
 
 size_t tc_workspace_bytes(const gatlas_matmul_desc *d, const Geometry &g) {
@@ -493,27 +542,34 @@ int matmul_tc(const gatlas_matmul_desc *d, const Geometry &g, const float *A, co
     if (!ws) {
         ws = device_scratch(pl.total);
         if (!ws) return set_error(GATLAS_ERR_NOMEM, "matmul: scratch of %zu bytes", pl.total);
-    } else if (ws_bytes < pl.total) {
-        return set_error(GATLAS_ERR_INVALID, "matmul: workspace %zu < %zu bytes", ws_bytes, pl.total);
-    } else if (!aligned_to(ws, 1024)) {
-        return set_error(GATLAS_ERR_INVALID, "matmul: workspace must be 1024-byte aligned");
+        ws_bytes = pl.total;
     }
-    uint8_t *base = static_cast<uint8_t *>(ws);
-    __nv_bfloat16 *ap[3] = {nullptr, nullptr, nullptr}, *bp[3] = {nullptr, nullptr, nullptr};
-    for (int i = 0; i < pl.np; ++i) {
-        ap[i] = reinterpret_cast<__nv_bfloat16 *>(base + i * pl.a_piece_bytes);
-        bp[i] = reinterpret_cast<__nv_bfloat16 *>(base + pl.np * pl.a_piece_bytes + i * pl.b_piece_bytes);
-    }
-    // A: K-major already when not transposed; B: K-major when transposed.
-    int rc = launch_split(pl.np, g.ta, A, g.M, g.K, pl.Kp, g.lda, g.stride_a, g.batch, ap, stream);
+    int rc = tc_prepare(d, g, A, B, ws, ws_bytes, stream);
     if (rc) return rc;
-    rc = launch_split(pl.np, !g.tb, B, g.N, g.K, pl.Kp, g.ldb, g.stride_b, g.batch, bp, stream);
-    if (rc) return rc;
-    switch (pl.mode) {
-        case 0: return launch_tc<0>(g, pl, ap, bp, C, d->alpha, d->beta, d->gemm, (int)d->extra, stream);
-        case 1: return launch_tc<1>(g, pl, ap, bp, C, d->alpha, d->beta, d->gemm, (int)d->extra, stream);
-        default: return launch_tc<2>(g, pl, ap, bp, C, d->alpha, d->beta, d->gemm, (int)d->extra, stream);
-    }
+    return tc_run(d, g, ws, ws_bytes, C, stream);
 }
 
 }  // namespace gatlas
+
+extern "C" int gatlas_matmul_tc_prepare(const gatlas_matmul_desc *d, const float *A, const float *B, void *workspace,
+                                        size_t workspace_bytes, void *stream) {
+    using namespace gatlas;
+    if (!d) return set_error(GATLAS_ERR_INVALID, "matmul_tc_prepare: null descriptor");
+    Geometry g;
+    if (!resolve_geometry(d, &g)) return set_error(GATLAS_ERR_INVALID, "matmul_tc_prepare: invalid dimensions");
+    if (!A || !B) return set_error(GATLAS_ERR_INVALID, "matmul_tc_prepare: null operand");
+    if (g.M == 0 || g.N == 0 || g.K == 0) return GATLAS_OK;
+    return tcg::tc_prepare(d, g, A, B, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+extern "C" int gatlas_matmul_tc_run(const gatlas_matmul_desc *d, const void *workspace, size_t workspace_bytes,
+                                    float *C, void *stream) {
+    using namespace gatlas;
+    if (!d) return set_error(GATLAS_ERR_INVALID, "matmul_tc_run: null descriptor");
+    Geometry g;
+    if (!resolve_geometry(d, &g)) return set_error(GATLAS_ERR_INVALID, "matmul_tc_run: invalid dimensions");
+    if (g.M == 0 || g.N == 0) return GATLAS_OK;
+    if (!C) return set_error(GATLAS_ERR_INVALID, "matmul_tc_run: null C");
+    if (g.batch > 65535) return set_error(GATLAS_ERR_INVALID, "matmul_tc_run: batch > 65535");
+    return tcg::tc_run(d, g, workspace, workspace_bytes, C, (cudaStream_t)stream);
+}

@@ -224,6 +224,11 @@ __global__ void __launch_bounds__(kGemvThreads)
 // ---------------------------------------------------------------------------
 // launch
 // ---------------------------------------------------------------------------
+template <typename T>
+static int matvec_image_dispatch(const gatlas_matvec_desc *, const T *, const T *, T *, cudaStream_t) {
+    return set_error(GATLAS_ERR_UNSUPPORTED, "matvec: image (TMA) engine not built yet");
+}
+
 struct ColsPlan {
     int vw;
     size_t ncb, nseg, seg_len, part_bytes, counter_bytes;
@@ -283,7 +288,8 @@ template <typename T>
 static int matvec_launch(const gatlas_matvec_desc *d, const T *A, const T *x, T *y, void *ws,
                          size_t ws_bytes, cudaStream_t stream) {
     if (!d) return set_error(GATLAS_ERR_INVALID, "matvec: null descriptor");
-    if (d->engine != GATLAS_ENGINE_BUFFER && d->engine != GATLAS_ENGINE_IMAGE)
+    if (d->engine == GATLAS_ENGINE_IMAGE) return matvec_image_dispatch<T>(d, A, x, y, stream);
+    if (d->engine != GATLAS_ENGINE_BUFFER)
         return set_error(GATLAS_ERR_INVALID, "matvec: engine %d is not buffer/image", d->engine);
     if (d->m == 0) return GATLAS_OK;
     if (!A || !x || !y) return set_error(GATLAS_ERR_INVALID, "matvec: null pointer");

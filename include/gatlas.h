@@ -151,6 +151,17 @@ int gatlas_matmul_f32(const gatlas_matmul_desc *d, const float *A, const float *
                       void *workspace, size_t workspace_bytes, void *stream);
 int gatlas_matmul_f64(const gatlas_matmul_desc *d, const double *A, const double *B, double *C,
                       void *workspace, size_t workspace_bytes, void *stream);
+/* Tensor-core engines in two steps, for operands that stay resident: prepare
+ * writes the BF16 pieces of A and B into the workspace
+ * (gatlas_matmul_workspace_size bytes, 1024-byte aligned); run contracts the
+ * prepared pieces into C and may be repeated.  gatlas_matmul_f32 with a TC_*
+ * engine is prepare followed by run.  No reference counterpart (the reference
+ * regenerates and re-uploads operands per run, KernelMatmulBuffer.hpp:83-171). */
+int gatlas_matmul_tc_prepare(const gatlas_matmul_desc *d, const float *A, const float *B, void *workspace,
+                             size_t workspace_bytes, void *stream);
+int gatlas_matmul_tc_run(const gatlas_matmul_desc *d, const void *workspace, size_t workspace_bytes, float *C,
+                         void *stream);
+
 /* 1 if a compiled kernel exists for (scalar 0=float/1=double, desc), else 0. */
 int gatlas_matmul_supported(int scalar, const gatlas_matmul_desc *d);
 
