@@ -21,7 +21,7 @@ HDRS    := $(wildcard include/*.h gatlas_b200/csrc/*.hpp gatlas_b200/csrc/*.cuh 
              gatlas_b200/csrc/kernels/*.hpp gatlas_b200/csrc/kernels/*.cuh gatlas_b200/csrc/host/*.hpp)
 
 CLI_SRC := $(wildcard gatlas_b200/cli/*.cpp)
-CLI_BIN := $(patsubst gatlas_b200/cli/%.cpp,$(BINDIR)/%,$(CLI_SRC))
+CLI_BIN := $(patsubst gatlas_b200/cli/%.cpp,$(BINDIR)/%,$(CLI_SRC)) $(BINDIR)/retry
 
 all: $(LIB) $(CLI_BIN) oracle
 
@@ -37,9 +37,15 @@ $(LIB): $(CU_OBJ) $(CPP_OBJ)
 	@mkdir -p $(LIBDIR)
 	$(NVCC) $(ARCH) -ccbin $(CXX_SYS) -shared -cudart static -o $@ $^ -lpthread -ldl -lrt
 
+# The tools link only against the library, whose statically linked CUDA
+# runtime they share (one runtime instance per process).
 $(BINDIR)/%: gatlas_b200/cli/%.cpp $(LIB) $(HDRS)
 	@mkdir -p $(BINDIR)
 	$(CXX_SYS) $(CXXFLAGS) -Igatlas_b200/csrc -o $@ $< -L$(LIBDIR) -lgatlas_b200 -Wl,-rpath,'$$ORIGIN/../lib'
+
+$(BINDIR)/retry: gatlas_b200/cli/retry
+	@mkdir -p $(BINDIR)
+	cp $< $@ && chmod +x $@
 
 oracle:
 	$(MAKE) -s -C oracle

@@ -69,3 +69,17 @@ extern "C" int gatlas_device_faults(int *flags, int clear) {
     if (flags) *flags = v;
     return GATLAS_OK;
 }
+
+extern "C" int gatlas_device_count(int *count) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (count) *count = (e == cudaSuccess) ? n : 0;
+    if (e != cudaSuccess) return gatlas::set_error(GATLAS_ERR_CUDA, "cudaGetDeviceCount: %s", cudaGetErrorString(e));
+    return GATLAS_OK;
+}
+
+extern "C" int gatlas_set_device(int device) {
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return gatlas::set_error(GATLAS_ERR_CUDA, "cudaSetDevice(%d): %s", device, cudaGetErrorString(e));
+    return GATLAS_OK;
+}

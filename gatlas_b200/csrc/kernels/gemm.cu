@@ -145,11 +145,10 @@ static int matmul_dispatch(const gatlas_matmul_desc *d, const T *A, const T *B, 
 // ---------------------------------------------------------------------------
 constexpr int kResTile = 32;
 
-__global__ void __launch_bounds__(256) residual_kernel(const float *A, const float *B, const float *C,
-                                                       int64_t M, int64_t N, int64_t K, int64_t lda,
-                                                       int64_t ldb, int64_t ldc, int ta, int tb,
-                                                       double alpha, double beta_unused, int gemm,
-                                                       double *stats) {
+__global__ void __launch_bounds__(256) residual_kernel(const float *A, const float *B, const float *Cin,
+                                                       const float *C, int64_t M, int64_t N, int64_t K,
+                                                       int64_t lda, int64_t ldb, int64_t ldc, int ta, int tb,
+                                                       double alpha, double beta, int gemm, double *stats) {
     __shared__ double As[kResTile][kResTile + 1];
     __shared__ double Bs[kResTile][kResTile + 1];
     __shared__ double red[3][256];
@@ -179,7 +178,8 @@ __global__ void __launch_bounds__(256) residual_kernel(const float *A, const flo
         for (int j = 0; j < 2; ++j) {
             const int64_t r = m0 + ty + 16 * i, c = n0 + tx + 16 * j;
             if (r < M && c < N) {
-                const double ref = gemm ? alpha * acc[i][j] : acc[i][j];
+                double ref = gemm ? alpha * acc[i][j] : acc[i][j];
+                if (gemm && Cin && beta != 0.0) ref += beta * (double)Cin[r * ldc + c];
                 const double dlt = (double)C[r * ldc + c] - ref;
                 s2 += dlt * dlt;
                 r2 += ref * ref;
@@ -187,7 +187,6 @@ __global__ void __launch_bounds__(256) residual_kernel(const float *A, const flo
                 mx = fmax(mx, fabs(dlt));
             }
         }
-    (void)beta_unused;
     red[0][threadIdx.x] = s2;
     red[1][threadIdx.x] = r2;
     red[2][threadIdx.x] = s1;
@@ -237,23 +236,17 @@ extern "C" int gatlas_matmul_supported(int scalar, const gatlas_matmul_desc *d) 
     return scalar == 0 && gatlas::tc_supported(d);
 }
 
-extern "C" int gatlas_matmul_residual_f32(const gatlas_matmul_desc *d, const float *A, const float *B,
-                                          const float *C, double *out_host, void *stream_) {
-    using namespace gatlas;
-    if (!d || !out_host) return set_error(GATLAS_ERR_INVALID, "residual: null argument");
-    Geometry g;
-    if (!resolve_geometry(d, &g)) return set_error(GATLAS_ERR_INVALID, "residual: invalid dimensions");
-    if (g.batch != 1) return set_error(GATLAS_ERR_INVALID, "residual: batch must be 1");
-    if (d->gemm && d->beta != 0.0)
-        return set_error(GATLAS_ERR_INVALID, "residual: beta must be 0 (C holds the product)");
-    cudaStream_t stream = (cudaStream_t)stream_;
+namespace gatlas {
+
+int matmul_residual(const Geometry &g, double alpha, double beta, int gemm, const float *A, const float *B,
+                    const float *Cin, const float *C, double *out_host, cudaStream_t stream) {
     double *stats = static_cast<double *>(device_scratch(4 * sizeof(double)));
     if (!stats) return set_error(GATLAS_ERR_NOMEM, "residual: scratch");
     cudaError_t e = cudaMemsetAsync(stats, 0, 4 * sizeof(double), stream);
     if (e != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "residual: %s", cudaGetErrorString(e));
     dim3 grid((unsigned)((g.N + kResTile - 1) / kResTile), (unsigned)((g.M + kResTile - 1) / kResTile));
-    residual_kernel<<<grid, 256, 0, stream>>>(A, B, C, g.M, g.N, g.K, g.lda, g.ldb, g.ldc, g.ta, g.tb,
-                                              d->alpha, d->beta, d->gemm, stats);
+    residual_kernel<<<grid, 256, 0, stream>>>(A, B, Cin, C, g.M, g.N, g.K, g.lda, g.ldb, g.ldc, g.ta, g.tb, alpha,
+                                              beta, gemm, stats);
     int rc = check_launch("residual_kernel");
     if (rc) return rc;
     double h[4];
@@ -265,4 +258,18 @@ extern "C" int gatlas_matmul_residual_f32(const gatlas_matmul_desc *d, const flo
     out_host[2] = h[2];
     out_host[3] = h[3];
     return GATLAS_OK;
+}
+
+}  // namespace gatlas
+
+extern "C" int gatlas_matmul_residual_f32(const gatlas_matmul_desc *d, const float *A, const float *B,
+                                          const float *C, double *out_host, void *stream_) {
+    using namespace gatlas;
+    if (!d || !out_host) return set_error(GATLAS_ERR_INVALID, "residual: null argument");
+    Geometry g;
+    if (!resolve_geometry(d, &g)) return set_error(GATLAS_ERR_INVALID, "residual: invalid dimensions");
+    if (g.batch != 1) return set_error(GATLAS_ERR_INVALID, "residual: batch must be 1");
+    if (d->gemm && d->beta != 0.0)
+        return set_error(GATLAS_ERR_INVALID, "residual: beta must be 0 (C holds the product)");
+    return matmul_residual(g, d->alpha, 0.0, d->gemm, A, B, nullptr, C, out_host, (cudaStream_t)stream_);
 }

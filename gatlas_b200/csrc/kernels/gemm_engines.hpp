@@ -20,6 +20,11 @@ struct Geometry {
 
 bool resolve_geometry(const gatlas_matmul_desc *d, Geometry *g);
 
+// FP64 residual of C against alpha*op(A)*op(B) (+ beta*Cin when gemm and Cin):
+// out = {||C-Cref||_F, ||Cref||_F, max|C-Cref|, sum|C-Cref|}; batch 1 geometry.
+int matmul_residual(const Geometry &g, double alpha, double beta, int gemm, const float *A, const float *B,
+                    const float *Cin, const float *C, double *out_host, cudaStream_t stream);
+
 // image engine: SIMT math on TMA tensor-map tile loads (gemm_image.cu)
 int matmul_image_f32(const gatlas_matmul_desc *d, const Geometry &g, const float *A, const float *B,
                      float *C, cudaStream_t stream);

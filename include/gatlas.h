@@ -181,6 +181,43 @@ int gatlas_fill_f64(double *out, size_t n, int dist, uint64_t seed, uint64_t off
 int gatlas_matmul_residual_f32(const gatlas_matmul_desc *d, const float *A, const float *B,
                                const float *C, double *out_host, void *stream);
 
+/* ---- plugin surface: KernelInterface objects -------------------------------
+ * One object per kernel family and -T type, with the reference's parameter
+ * vector, validity rules, names, flop counts and work-item shapes
+ * (KernelInterface, GatlasBenchmark.hpp:28-58; KernelBase{Matmul,Matvec,
+ * Saxpy}).  op is "matmul", "matvec" or "saxpy"; type is a -T name of the
+ * reference's tools (float1|float2|float4|double1|double2|double4|floatimg|
+ * doubleimg), or tcbf16|split3|split6 for the tensor-core matmul engines.
+ * String and vector getters return the full length and copy at most
+ * len - 1 characters / cap elements. */
+typedef struct gatlas_kernel gatlas_kernel;
+int gatlas_kernel_create(const char *op, const char *type, gatlas_kernel **out);
+void gatlas_kernel_destroy(gatlas_kernel *k);
+size_t gatlas_kernel_name(const gatlas_kernel *k, char *buf, size_t len);          /* kernelName */
+int gatlas_kernel_set_params(gatlas_kernel *k, const size_t *params, size_t n);    /* setParams */
+/* getParams: returns 1 and the vector when the point is valid (validParams), else 0 */
+int gatlas_kernel_get_params(const gatlas_kernel *k, size_t *params, size_t cap, size_t *n);
+size_t gatlas_kernel_number_flops(const gatlas_kernel *k);                          /* numberFlops */
+size_t gatlas_kernel_total_variations(const gatlas_kernel *k);
+size_t gatlas_kernel_extra_param_detail(const gatlas_kernel *k, size_t *out, size_t cap);
+size_t gatlas_kernel_global_work_items(const gatlas_kernel *k, size_t *out, size_t cap);
+size_t gatlas_kernel_local_work_items(const gatlas_kernel *k, size_t *out, size_t cap);
+size_t gatlas_kernel_print(const gatlas_kernel *k, char *buf, size_t len);         /* print */
+void gatlas_kernel_paranoid_check(gatlas_kernel *k);                                /* paranoidCheck */
+/* Bench::run (GatlasBenchmark.cpp:178-289): set params, journal the build and
+ * run states when `journal` is a path, set args, time `trials` launches (with
+ * the host<->device copies when bus_to_device / bus_from_device), check the
+ * output.  *usec = elapsed microseconds, 0 when the point failed. */
+int gatlas_bench_run(gatlas_kernel *k, const char *journal, size_t trials, const size_t *params, size_t n,
+                     int bus_to_device, int bus_from_device, size_t *usec);
+
+/* ---- devices --------------------------------------------------------------
+ * Device selection for callers that do not link the CUDA runtime themselves
+ * (the library carries its own).  Replaces the reference's device choice by
+ * -d cpu|gpu|accN (GatlasAppUtil.cpp:30-60). */
+int gatlas_device_count(int *count);
+int gatlas_set_device(int device);
+
 /* ---- device faults ------------------------------------------------------
  * Kernels that wait on asynchronous copies (mbarrier waits) give up after a
  * bounded number of polls, set a bit in the current device's fault word and

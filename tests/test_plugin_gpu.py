@@ -1,0 +1,98 @@
+"""The plugin layer and the tools on the GPU: Bench::run with the journal,
+the reference's test pattern and paranoid checks, and short searches."""
+import os
+import subprocess
+
+import pytest
+
+from gatlas_b200.plugin import Kernel
+from oracle.params import BUILD_IN_PROGRESS, BUILD_OK, RUN_IN_PROGRESS, RUN_OK, journal_key
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BIN = os.path.join(ROOT, "gatlas_b200", "bin")
+
+
+def run(args):
+    return subprocess.run([os.path.join(BIN, args[0])] + args[1:], capture_output=True, text=True, timeout=600)
+
+
+@pytest.mark.parametrize("paranoid", [False, True])
+@pytest.mark.parametrize("t,p", [
+    ("float4", [1, 0, 512, 512, 512, 0, 0, 16, 16, 8, 4, 0]),
+    ("float4", [2, 1, 256, 256, 256, 1, 1, 16, 16, 8, 4, 5]),
+    ("double2", [1, 1, 256, 256, 256, 0, 1, 16, 16, 4, 4, 0]),
+    ("split3", [1, 0, 512, 512, 512, 0, 0, 16, 16, 8, 4, 0]),
+    ("split6", [1, 1, 256, 256, 256, 1, 0, 16, 16, 8, 4, 0]),
+    ("tcbf16", [1, 0, 256, 512, 128, 0, 1, 16, 16, 8, 4, 0]),
+])
+def test_bench_run_journal_and_checks(cuda, tmp_path, t, p, paranoid):
+    k = Kernel("matmul", t)
+    if paranoid:
+        k.paranoid_check()
+    j = tmp_path / "run.journal"
+    usec = k.bench_run(p, journal=str(j))
+    assert usec > 0                     # test pattern C == K, or paranoid check passed
+    key = journal_key(k.kernel_name(), p)
+    lines = [ln.split("\t") for ln in j.read_text().splitlines()]
+    assert [ln[0] for ln in lines] == [key] * 5
+    assert [int(ln[1]) for ln in lines] == [BUILD_IN_PROGRESS, BUILD_OK, RUN_IN_PROGRESS, RUN_OK, usec]
+
+
+@pytest.mark.parametrize("op,t,p", [
+    ("matvec", "float4", [1, 0, 4096, 4096, 0, 64, 4, 4, 0]),
+    ("matvec", "float4", [1, 1, 4096, 2048, 1, 64, 8, 4, 1]),
+    ("matvec", "double2", [2, 0, 1024, 512, 1, 64, 2, 2, 0]),
+    ("saxpy", "float4", [1, 1 << 20, 4, 256, 0, 4, 0, 4, 0]),
+    ("saxpy", "double2", [1, 1 << 18, 2, 64, 0, 2, 0, 2, 1]),
+])
+@pytest.mark.parametrize("paranoid", [False, True])
+def test_bench_run_matvec_saxpy(cuda, op, t, p, paranoid):
+    k = Kernel(op, t)
+    if paranoid:
+        k.paranoid_check()
+    assert k.bench_run(p, bus_to_device=True, bus_from_device=True) > 0
+
+
+def test_unsupported_point_is_bad_on_resume(cuda, tmp_path):
+    k = Kernel("matmul", "float4")
+    p = [1, 0, 640, 640, 640, 0, 0, 10, 10, 8, 4, 0]    # valid for the reference, not compiled here
+    j = tmp_path / "bad.journal"
+    assert k.bench_run(p, journal=str(j)) == 0
+    assert j.read_text().splitlines()[-1] == f"{journal_key(k.kernel_name(), p)}\t{BUILD_IN_PROGRESS}"
+
+
+def test_bench_matmul_search_and_paranoid(cuda, tmp_path):
+    j = tmp_path / "mm.journal"
+    r = run(["bench_matmul", "-d", "gpu0", "-j", str(j), "-T", "float4", "-n", "512", "-g", "16", "-y", "8",
+             "-t", "2", "-p"])
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip().endswith("***DONE***")
+    assert "absdiff: 0" in r.stderr and "fail" not in r.stderr
+    final = [ln for ln in r.stdout.splitlines() if ln.startswith("[") and " usec\tavg: " in ln]
+    assert len(final) == 12
+    # resume: every point is now journaled and replayed
+    r2 = run(["bench_matmul", "-d", "gpu0", "-j", str(j), "-T", "float4", "-n", "512", "-g", "16", "-y", "8",
+              "-t", "2"])
+    assert r2.returncode == 0
+    final2 = [ln for ln in r2.stdout.splitlines() if ln.startswith("[") and " usec\tavg: " in ln]
+    assert final2 == final
+
+
+def test_bench_matmul_em_search(cuda, tmp_path):
+    j = tmp_path / "em.journal"
+    r = run(["bench_matmul", "-d", "gpu0", "-j", str(j), "-T", "float4", "-n", "1024", "-e", "-t", "2"])
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip().endswith("***DONE***")
+    assert " usec\tavg: " in r.stdout
+
+
+def test_bench_matvec_and_saxpy_tools(cuda, tmp_path):
+    r = run(["bench_matvec", "-d", "gpu0", "-j", str(tmp_path / "mv.journal"), "-T", "float4", "-n", "4096",
+             "-g", "64", "-y", "4", "-p"])
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip().endswith("***DONE***") and " usec\tavg: " in r.stdout
+    r = run(["bench_saxpy", "-d", "gpu0", "-j", str(tmp_path / "sx.journal"), "-T", "float4", "-m", "262144",
+             "-w", "3", "-t", "2", "-p"])
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip().endswith("***DONE***") and "absdiff: 0" in r.stderr
