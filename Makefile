@@ -14,7 +14,7 @@ BINDIR  := gatlas_b200/bin
 LIB     := $(LIBDIR)/libgatlas_b200.so
 
 CU_SRC  := $(wildcard gatlas_b200/csrc/*.cu gatlas_b200/csrc/kernels/*.cu)
-CPP_SRC := $(wildcard gatlas_b200/csrc/*.cpp gatlas_b200/csrc/host/*.cpp)
+CPP_SRC := $(wildcard gatlas_b200/csrc/*.cpp gatlas_b200/csrc/host/*.cpp gatlas_b200/csrc/kernels/*.cpp)
 CU_OBJ  := $(patsubst %.cu,$(BUILD)/%.o,$(CU_SRC))
 CPP_OBJ := $(patsubst %.cpp,$(BUILD)/%.o,$(CPP_SRC))
 HDRS    := $(wildcard include/*.h gatlas_b200/csrc/*.hpp gatlas_b200/csrc/*.cuh \
@@ -32,6 +32,16 @@ $(BUILD)/%.o: %.cu $(HDRS)
 $(BUILD)/%.o: %.cpp $(HDRS)
 	@mkdir -p $(dir $@)
 	$(CXX_SYS) $(CXXFLAGS) -c $< -o $@
+
+# The SIMT kernel template embedded as a string for run-time compilation.
+GEN := $(BUILD)/gen
+$(GEN)/gemm_simt_source.inc: gatlas_b200/csrc/kernels/gemm_simt.cuh
+	@mkdir -p $(GEN)
+	( printf 'R"GATLAS_SRC('; cat $<; printf ')GATLAS_SRC"\n' ) > $@
+
+$(BUILD)/gatlas_b200/csrc/kernels/jit.o: gatlas_b200/csrc/kernels/jit.cpp $(GEN)/gemm_simt_source.inc $(HDRS)
+	@mkdir -p $(dir $@)
+	$(CXX_SYS) $(CXXFLAGS) -I$(GEN) -c $< -o $@
 
 $(LIB): $(CU_OBJ) $(CPP_OBJ)
 	@mkdir -p $(LIBDIR)

@@ -234,8 +234,9 @@ def matmul_tc_run(workspace, M, N, K, C, trans_a=False, trans_b=False, engine="t
 
 
 def matmul_supported(engine="buffer", tile=None, trans_a=False, trans_b=False, double=False):
+    """1: prebuilt kernel; 2: compiled at run time on first use; 0: cannot run."""
     d = matmul_desc(1, 1, 1, trans_a, trans_b, engine=engine, tile=tile)
-    return bool(lib().gatlas_matmul_supported(int(double), ctypes.byref(d)))
+    return int(lib().gatlas_matmul_supported(int(double), ctypes.byref(d)))
 
 
 def matmul_workspace_size(M, N, K, engine, trans_a=False, trans_b=False, batch=1) -> int:

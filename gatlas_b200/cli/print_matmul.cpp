@@ -96,6 +96,9 @@ int main(int argc, char **argv) {
         exit(1);
     }
     cout << k;
-    cout << "// compiled into the library: " << (k.build() ? "yes" : "no") << endl;
+    const int level = k.supportLevel();
+    cout << "// " << (level == 1 ? "prebuilt in the library" : level == 2 ? "compiled at run time (NVRTC) on first use"
+                                                                          : "no kernel for this point")
+         << endl;
     return 0;
 }

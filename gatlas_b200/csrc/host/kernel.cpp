@@ -9,6 +9,7 @@
 
 #include "../../../include/gatlas.h"
 #include "../kernels/gemm_engines.hpp"
+#include "../kernels/jit.hpp"
 #include "../kernels/reference.hpp"
 
 namespace gatlas {
@@ -181,11 +182,33 @@ bool KernelMatmul::build() {
         return false;
     }
     const gatlas_matmul_desc d = matmul_desc_of(*this, variant_, vl_, alpha_, beta_);
-    if (!gatlas_matmul_supported(scalar_ == Scalar::Double, &d)) {
-        std::cerr << "error: no compiled kernel for this point";
+    const int support = gatlas_matmul_supported(scalar_ == Scalar::Double, &d);
+    if (support == 0) {
+        std::cerr << "error: no kernel for this point";
         return false;
     }
+    if (support == 2) {
+        // no prebuilt instantiation: compile it now, as the reference builds
+        // its OpenCL program for every point (GatlasBenchmark.cpp:286-301)
+        void *fn = nullptr;
+        if (jit::simt_function(jit_point(), &fn) != GATLAS_OK) {
+            char buf[512];
+            gatlas_last_error(buf, sizeof(buf));
+            std::cerr << "error: " << buf;
+            return false;
+        }
+    }
     return true;
+}
+
+int KernelMatmul::supportLevel() const {
+    const gatlas_matmul_desc d = matmul_desc_of(*this, variant_, vl_, alpha_, beta_);
+    return gatlas_matmul_supported(scalar_ == Scalar::Double, &d);
+}
+
+jit::Point KernelMatmul::jit_point() const {
+    return jit::Point{scalar_ == Scalar::Double ? 1 : 0, transposeA() ? 1 : 0, transposeB() ? 1 : 0,
+                      (int)groupHeight(), (int)groupWidth(), (int)blockHeight(), (int)blockWidth(), (int)vl_};
 }
 
 bool KernelMatmul::setArgs(bool syncInput) {
@@ -328,6 +351,7 @@ std::ostream &KernelMatmul::print(std::ostream &os) const {
         for (size_t i = 0; i < x.size(); ++i) os << (i ? " " : "") << x[i];
         os << ") [inlineMNK, loopOrder" << (variant_ == Variant::Image ? ", globalID" : "")
            << "]: recorded; every order accumulates k = 0..K-1 in sequence\n";
+        if (variant_ == Variant::Buffer) os << "\n" << jit::simt_source(jit_point());
     }
     return os;
 }

@@ -18,6 +18,7 @@
 #include <string>
 #include <vector>
 
+#include "../kernels/jit.hpp"
 #include "params.hpp"
 
 namespace gatlas {
@@ -89,9 +90,12 @@ class KernelMatmul : public KernelInterface, public MatmulParams {
     Variant variant() const { return variant_; }
     size_t vectorLength() const { return vl_; }
     double lastAbsdiff() const { return absdiff_; }
+    // 1: prebuilt kernel, 2: compiled at run time on first use, 0: cannot run
+    int supportLevel() const;
 
   private:
     size_t elem() const { return scalar_ == Scalar::Float ? 4 : 8; }
+    jit::Point jit_point() const;
     Scalar scalar_;
     Variant variant_;
     size_t vl_;

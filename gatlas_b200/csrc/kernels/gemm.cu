@@ -9,7 +9,9 @@
 #include "../common.cuh"
 #include "../device_state.cuh"
 #include "gemm_engines.hpp"
+#include "gemm_simt.cuh"
 #include "gemm_simt_registry.hpp"
+#include "jit.hpp"
 
 namespace gatlas {
 
@@ -65,6 +67,35 @@ static int feasible_vl(const Geometry &g, const void *A, const void *B, size_t e
     return 1;
 }
 
+// A point without a prebuilt instantiation: compile it at run time.
+template <typename T>
+static int matmul_simt_jit(const gatlas_matmul_desc *d, const Geometry &g, const T *A, const T *B, T *C,
+                           const jit::Point &pt, cudaStream_t stream) {
+    void *fn = nullptr;
+    const int rc = jit::simt_function(pt, &fn);
+    if (rc) return rc;
+    simt::GemmArgs<T> a;
+    a.A = A;
+    a.B = B;
+    a.C = C;
+    a.M = g.M;
+    a.N = g.N;
+    a.K = g.K;
+    a.lda = g.lda;
+    a.ldb = g.ldb;
+    a.ldc = g.ldc;
+    a.stride_a = g.stride_a;
+    a.stride_b = g.stride_b;
+    a.stride_c = g.stride_c;
+    a.alpha = (T)d->alpha;
+    a.beta = (T)d->beta;
+    a.gemm = d->gemm;
+    const int64_t BM = (int64_t)pt.gh * pt.bh, BN = (int64_t)pt.gw * pt.bw;
+    const int64_t gx = (g.N + BN - 1) / BN, gy = (g.M + BM - 1) / BM;
+    if (gx > 0x7fffffff || gy > 65535) return set_error(GATLAS_ERR_INVALID, "matmul: grid too large");
+    return jit::launch(fn, (unsigned)gx, (unsigned)gy, (unsigned)g.batch, (unsigned)(pt.gh * pt.gw), &a, stream);
+}
+
 template <typename T>
 static int matmul_simt(const gatlas_matmul_desc *d, const Geometry &g, const T *A, const T *B, T *C,
                        cudaStream_t stream) {
@@ -92,10 +123,7 @@ static int matmul_simt(const gatlas_matmul_desc *d, const Geometry &g, const T *
         for (int v = vl; v >= 1 && !e; v /= 2) e = simt::find(scalar, g.ta, g.tb, gh, gw, bh, bw, v);
         if (!e) e = simt::find(scalar, g.ta, g.tb, 16, 16, 4, 4, 1);
     }
-    if (!e)
-        return set_error(GATLAS_ERR_UNSUPPORTED,
-                         "matmul: no compiled SIMT kernel for %s tA=%d tB=%d group %dx%d block %dx%d vl %d",
-                         scalar ? "double" : "float", (int)g.ta, (int)g.tb, gh, gw, bh, bw, vl);
+    if (!e) return matmul_simt_jit<T>(d, g, A, B, C, jit::Point{scalar, g.ta, g.tb, gh, gw, bh, bw, vl}, stream);
     simt::LaunchArgs l;
     l.A = A;
     l.B = B;
@@ -229,8 +257,12 @@ extern "C" int gatlas_matmul_supported(int scalar, const gatlas_matmul_desc *d) 
     if (d->engine == GATLAS_ENGINE_BUFFER) {
         if (d->group_h == 0 && d->group_w == 0 && d->block_h == 0 && d->block_w == 0) return 1;
         const int vl = d->vector_length ? (int)d->vector_length : 1;
-        return gatlas::simt::find(scalar, d->trans_a != 0, d->trans_b != 0, (int)d->group_h, (int)d->group_w,
-                                  (int)d->block_h, (int)d->block_w, vl) != nullptr;
+        if (gatlas::simt::find(scalar, d->trans_a != 0, d->trans_b != 0, (int)d->group_h, (int)d->group_w,
+                               (int)d->block_h, (int)d->block_w, vl) != nullptr)
+            return 1;
+        const gatlas::jit::Point pt{scalar, d->trans_a != 0, d->trans_b != 0, (int)d->group_h, (int)d->group_w,
+                                    (int)d->block_h, (int)d->block_w, vl};
+        return gatlas::jit::available() && gatlas::jit::point_ok(pt) ? 2 : 0;
     }
     if (d->engine == GATLAS_ENGINE_IMAGE) return gatlas::image_supported(scalar, d);
     return scalar == 0 && gatlas::tc_supported(d);

@@ -27,9 +27,16 @@
 // works; the reference's divisibility rules are enforced above this layer.
 #pragma once
 
+// This header is also compiled at run time by NVRTC (for parameter points
+// without a prebuilt instantiation), where no system headers are available.
+#ifndef __CUDACC_RTC__
 #include <cuda_runtime.h>
 #include <stddef.h>
 #include <stdint.h>
+#else
+typedef long long int64_t;
+typedef unsigned long long uintptr_t;
+#endif
 
 namespace gatlas {
 namespace simt {
@@ -78,7 +85,10 @@ struct Tile {
     static constexpr int LA = (A_VECS + NT - 1) / NT;
     static constexpr int LB = (B_VECS + NT - 1) / NT;
     static constexpr int SMEM_ELEMS = 2 * BK * (LDA_S + LDB_S);
-    static_assert(BK % VL == 0 && BM % VL == 0 && BN % VL == 0, "vector width must divide the tile");
+    // vectors run along each operand's contiguous dimension
+    static_assert(BK % VL == 0, "vector width must divide the K step");
+    static_assert(!TA || BM % VL == 0, "vector width must divide the A tile rows");
+    static_assert(TB || BN % VL == 0, "vector width must divide the B tile columns");
 };
 
 // FP32 points are capped at 128 registers so that 512 threads fit per SM.

@@ -35,6 +35,8 @@ namespace gatlas {
 namespace tcg {
 
 constexpr int BM = 128, BN = 256, BK = 32;
+constexpr int kGroupM = 16;  // tile rows per raster group
+
 // Default promotion interval: 4 slices of BK = 32, i.e. K = 128 per
 // TMEM segment (selectable per call through the descriptor's extra field).
 constexpr int kDefaultSegKblocks = 4;
@@ -111,7 +113,21 @@ __global__ void __launch_bounds__(kThreads2, 1)
     __shared__ int kb_issued, kb_consumed;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN, z = blockIdx.z;
+    // Grouped raster: consecutive CTAs walk kGroupM tile rows before moving to
+    // the next tile column, so that a wave of resident CTAs shares A and B
+    // tiles through L2 instead of re-reading all of B from DRAM every wave.
+    int tile_m, tile_n;
+    {
+        const int tiles_n = gridDim.x, tiles_m = gridDim.y;
+        const int bid = blockIdx.y * tiles_n + blockIdx.x;
+        const int per_group = kGroupM * tiles_n;
+        const int first_m = (bid / per_group) * kGroupM;
+        const int gm = min(tiles_m - first_m, kGroupM);
+        const int r = bid % per_group;
+        tile_m = first_m + r % gm;
+        tile_n = r / gm;
+    }
+    const int m0 = tile_m * BM, n0 = tile_n * BN, z = blockIdx.z;
     const CUtensorMap *tA[3] = {&ta0, &ta1, &ta2};
     const CUtensorMap *tB[3] = {&tb0, &tb1, &tb2};
     const int nseg = (p.kblocks + p.seg_kblocks - 1) / p.seg_kblocks;

@@ -162,7 +162,9 @@ int gatlas_matmul_tc_prepare(const gatlas_matmul_desc *d, const float *A, const 
 int gatlas_matmul_tc_run(const gatlas_matmul_desc *d, const void *workspace, size_t workspace_bytes, float *C,
                          void *stream);
 
-/* 1 if a compiled kernel exists for (scalar 0=float/1=double, desc), else 0. */
+/* 1 if a prebuilt kernel exists for (scalar 0=float/1=double, desc); 2 if
+ * the SIMT point has no prebuilt instantiation but will be compiled on first
+ * use (NVRTC, cached per device); 0 if it cannot run. */
 int gatlas_matmul_supported(int scalar, const gatlas_matmul_desc *d);
 
 /* ---- data generation and residuals ---------------------------------------

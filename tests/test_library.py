@@ -55,8 +55,11 @@ def test_compiled_simt_points_cover_the_tuning_grid():
             for bh in (4, 8):
                 for bw in (4, 8):
                     for vl in (1, 2, 4):
-                        assert g.matmul_supported("buffer", (gh, gw, bh, bw, vl))
-    assert not g.matmul_supported("buffer", (10, 10, 7, 4, 4))
+                        assert g.matmul_supported("buffer", (gh, gw, bh, bw, vl)) == 1
+    # other points of the reference's space are compiled at run time
+    assert g.matmul_supported("buffer", (10, 10, 7, 4, 4)) == 2
+    assert g.matmul_supported("buffer", (9, 9, 5, 4, 4), trans_a=True) == 0   # 45 rows not a multiple of 4
+    assert g.matmul_supported("buffer", (8, 8, 4, 4, 3)) == 0
 
 
 def test_workspace_queries():

@@ -54,12 +54,23 @@ def test_bench_run_matvec_saxpy(cuda, op, t, p, paranoid):
     assert k.bench_run(p, bus_to_device=True, bus_from_device=True) > 0
 
 
-def test_unsupported_point_is_bad_on_resume(cuda, tmp_path):
+def test_run_time_compiled_point(cuda, tmp_path):
+    # a point of the reference's space without a prebuilt kernel is compiled at
+    # build time and checked like any other (paranoid: bit-exact vs the fmaf chain)
     k = Kernel("matmul", "float4")
-    p = [1, 0, 640, 640, 640, 0, 0, 10, 10, 8, 4, 0]    # valid for the reference, not compiled here
-    j = tmp_path / "bad.journal"
-    assert k.bench_run(p, journal=str(j)) == 0
-    assert j.read_text().splitlines()[-1] == f"{journal_key(k.kernel_name(), p)}\t{BUILD_IN_PROGRESS}"
+    k.paranoid_check()
+    p = [1, 1, 640, 640, 640, 1, 0, 10, 10, 8, 4, 7]
+    j = tmp_path / "jit.journal"
+    usec = k.bench_run(p, journal=str(j))
+    assert usec > 0
+    states = [int(ln.split("\t")[1]) for ln in j.read_text().splitlines()]
+    assert states == [BUILD_IN_PROGRESS, BUILD_OK, RUN_IN_PROGRESS, RUN_OK, usec]
+
+
+def test_double_odd_point_compiles(cuda):
+    k = Kernel("matmul", "double1")
+    k.paranoid_check()
+    assert k.bench_run([1, 1, 640, 640, 640, 0, 0, 8, 8, 10, 1, 2]) > 0   # docs/EXAMPLES:136 point
 
 
 def test_bench_matmul_search_and_paranoid(cuda, tmp_path):
