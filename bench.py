@@ -54,9 +54,9 @@ def _peaks():
                 "source": "fallback"}
 
 
-# DRAM bytes per launch of the split3 contraction at 8192^3 from an ncu capture
-# (None until captured); see profiles/.
-TC_TRAFFIC_BYTES = None
+# DRAM bytes (read + write) per launch of the split3 contraction at 8192^3,
+# from an ncu capture of the full-size launch (profiles/tc_gemm_kernel_split3_8192.md)
+TC_TRAFFIC_BYTES = 2.28e9 + 0.2555e9
 
 # nominal FP32 SIMT peak: 148 SMs x 128 FP32 lanes x 2 flop x 1.965 GHz
 FP32_SIMT_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12

@@ -106,9 +106,25 @@ def test_dgemm_bit_exact(cuda, ta, tb):
 
 
 def test_unsupported_point_reports(cuda):
+    # a vector width of 3 divides no K step: no kernel can be built for it
     with pytest.raises(g.GatlasError) as e:
-        _mm(cuda, np.ones(16, np.float32), np.ones(16, np.float32), 4, 4, 4, tile=(10, 10, 7, 4, 4))
-    assert e.value.status == g.ERR_UNSUPPORTED
+        _mm(cuda, np.ones(36, np.float32), np.ones(36, np.float32), 6, 6, 6, tile=(8, 8, 4, 4, 3))
+    assert e.value.status in (g.ERR_UNSUPPORTED, g.ERR_INVALID)
+
+
+@pytest.mark.parametrize("ta,tb", [(0, 0), (1, 0), (0, 1), (1, 1)])
+@pytest.mark.parametrize("tile", [(10, 10, 8, 4, 4), (9, 9, 4, 4, 4), (8, 8, 10, 1, 1), (10, 10, 12, 2, 2)])
+def test_run_time_compiled_points_bit_exact(cuda, ta, tb, tile):
+    # points of the reference's space outside the prebuilt grid (odd work
+    # groups, blockings up to 12) are compiled with NVRTC on first use
+    gh, gw, bh, bw, vl = tile
+    if ta and (gh * bh) % vl:
+        pytest.skip("not a valid point for transposed A")
+    M, N, K = gh * bh * 2, gw * bw * 3, 72
+    A = oracle.uniform(M * K, seed=gh + bh)
+    B = oracle.uniform(K * N, seed=gw + bw)
+    C = _mm(cuda, A, B, M, N, K, ta, tb, tile=tile)
+    assert np.array_equal(C, oracle.matmul(A, B, M, N, K, ta, tb, mode=oracle.FMA))
 
 
 def test_full_size_residual_4096(cuda):
