@@ -224,9 +224,19 @@ __global__ void __launch_bounds__(kGemvThreads)
 // ---------------------------------------------------------------------------
 // launch
 // ---------------------------------------------------------------------------
+int matvec_image_f32(const gatlas_matvec_desc *d, const float *A, const float *x, float *y, void *ws,
+                     size_t ws_bytes, cudaStream_t stream);
+size_t matvec_image_ws_bytes(const gatlas_matvec_desc *d);
+
 template <typename T>
-static int matvec_image_dispatch(const gatlas_matvec_desc *, const T *, const T *, T *, cudaStream_t) {
-    return set_error(GATLAS_ERR_UNSUPPORTED, "matvec: image (TMA) engine not built yet");
+static int matvec_image_dispatch(const gatlas_matvec_desc *d, const T *A, const T *x, T *y, void *ws,
+                                 size_t ws_bytes, cudaStream_t stream) {
+    if constexpr (sizeof(T) == 4) {
+        return matvec_image_f32(d, A, x, y, ws, ws_bytes, stream);
+    } else {
+        (void)d, (void)A, (void)x, (void)y, (void)ws, (void)ws_bytes, (void)stream;
+        return set_error(GATLAS_ERR_UNSUPPORTED, "matvec: the image (TMA) engine takes float operands");
+    }
 }
 
 struct ColsPlan {
@@ -288,7 +298,7 @@ template <typename T>
 static int matvec_launch(const gatlas_matvec_desc *d, const T *A, const T *x, T *y, void *ws,
                          size_t ws_bytes, cudaStream_t stream) {
     if (!d) return set_error(GATLAS_ERR_INVALID, "matvec: null descriptor");
-    if (d->engine == GATLAS_ENGINE_IMAGE) return matvec_image_dispatch<T>(d, A, x, y, stream);
+    if (d->engine == GATLAS_ENGINE_IMAGE) return matvec_image_dispatch<T>(d, A, x, y, ws, ws_bytes, stream);
     if (d->engine != GATLAS_ENGINE_BUFFER)
         return set_error(GATLAS_ERR_INVALID, "matvec: engine %d is not buffer/image", d->engine);
     if (d->m == 0) return GATLAS_OK;
@@ -375,7 +385,8 @@ extern "C" size_t gatlas_matvec_workspace_size(const gatlas_matvec_desc *d) {
         if (a > best) best = a;
         if (b > best) best = b;
     }
-    return best;
+    const size_t img = gatlas::matvec_image_ws_bytes(d);
+    return img > best ? img : best;
 }
 
 extern "C" int gatlas_matvec_f32(const gatlas_matvec_desc *d, const float *A, const float *x, float *y,

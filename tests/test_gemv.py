@@ -103,3 +103,52 @@ def test_full_size_16384(cuda, ta):
     ref = (A64[:, rows].T if ta else A64[rows]) @ x.double()
     err = torch.linalg.norm(y[rows].double() - ref) / torch.linalg.norm(ref)
     assert float(err) <= 4 * N * U32
+
+
+# ---- image engine (TMA tensor-map tiles) ----------------------------------------
+
+@pytest.mark.parametrize("ta", [0, 1])
+@pytest.mark.parametrize("M,N", [(4, 4), (16, 256), (100, 260), (1024, 4096), (4096, 1000), (333 * 4, 777 * 4),
+                                 (16384, 512)])
+def test_image_engine_tolerance(cuda, ta, M, N):
+    A = oracle.uniform(M * N, seed=M + 13 * N)
+    x = oracle.uniform(N, seed=N + 5)
+    y = _matvec(cuda, A, x, M, N, ta, engine="image")
+    ref = oracle.matvec(A, x, M, N, ta, mode=oracle.F64)
+    assert oracle.normwise_error(y, ref) <= 4 * N * U32
+
+
+@pytest.mark.parametrize("ta", [0, 1])
+def test_image_engine_known_answer_and_gemv(cuda, ta):
+    M, N = 2048, 4096
+    y = _matvec(cuda, np.ones(M * N, np.float32), np.ones(N, np.float32), M, N, ta, engine="image")
+    assert oracle.check_pattern(y, float(N))
+    A = oracle.uniform(M * N, seed=21)
+    x = oracle.uniform(N, seed=22)
+    yin = oracle.uniform(M, seed=23)
+    y = _matvec(cuda, A, x, M, N, ta, engine="image", gemv=True, yin=yin, alpha=1.5, beta=-0.25)
+    ref = oracle.matvec(A, x, M, N, ta, mode=oracle.F64, gemv=1, cin=yin, alpha=1.5, beta=-0.25)
+    assert oracle.normwise_error(y, ref) <= 4 * N * U32
+
+
+def test_image_engine_rejects_unaligned_rows(cuda):
+    with pytest.raises(g.GatlasError) as e:
+        _matvec(cuda, np.ones(33 * 65, np.float32), np.ones(65, np.float32), 33, 65, 0, engine="image")
+    assert e.value.status == g.ERR_UNSUPPORTED
+    assert g.device_faults() == 0
+
+
+@pytest.mark.parametrize("ta", [0, 1])
+def test_image_engine_full_size_matches_buffer(cuda, ta):
+    import torch
+    M = N = 16384
+    A = torch.empty(M * N, dtype=torch.float32, device=cuda)
+    x = torch.empty(N, dtype=torch.float32, device=cuda)
+    g.fill(A, "uniform", seed=31)
+    g.fill(x, "uniform", seed=32)
+    yb = g.matvec(A, x, M, N, trans_a=ta, engine="buffer")
+    yi = g.matvec(A, x, M, N, trans_a=ta, engine="image")
+    torch.cuda.synchronize()
+    err = torch.linalg.norm((yi - yb).double()) / torch.linalg.norm(yb.double())
+    assert float(err) <= 4 * N * U32
+    assert g.device_faults() == 0
