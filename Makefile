@@ -39,7 +39,12 @@ $(GEN)/gemm_simt_source.inc: gatlas_b200/csrc/kernels/gemm_simt.cuh
 	@mkdir -p $(GEN)
 	( printf 'R"GATLAS_SRC('; cat $<; printf ')GATLAS_SRC"\n' ) > $@
 
-$(BUILD)/gatlas_b200/csrc/kernels/jit.o: gatlas_b200/csrc/kernels/jit.cpp $(GEN)/gemm_simt_source.inc $(HDRS)
+$(GEN)/gemm_image_source.inc: gatlas_b200/csrc/kernels/gemm_image.cuh
+	@mkdir -p $(GEN)
+	( printf 'R"GATLAS_SRC('; cat $<; printf ')GATLAS_SRC"\n' ) > $@
+
+$(BUILD)/gatlas_b200/csrc/kernels/jit.o: gatlas_b200/csrc/kernels/jit.cpp $(GEN)/gemm_simt_source.inc \
+		$(GEN)/gemm_image_source.inc $(HDRS)
 	@mkdir -p $(dir $@)
 	$(CXX_SYS) $(CXXFLAGS) -I$(GEN) -c $< -o $@
 

@@ -208,7 +208,8 @@ int KernelMatmul::supportLevel() const {
 
 jit::Point KernelMatmul::jit_point() const {
     return jit::Point{scalar_ == Scalar::Double ? 1 : 0, transposeA() ? 1 : 0, transposeB() ? 1 : 0,
-                      (int)groupHeight(), (int)groupWidth(), (int)blockHeight(), (int)blockWidth(), (int)vl_};
+                      (int)groupHeight(), (int)groupWidth(), (int)blockHeight(), (int)blockWidth(),
+                      variant_ == Variant::Image ? 0 : (int)vl_, variant_ == Variant::Image ? 1 : 0};
 }
 
 bool KernelMatmul::setArgs(bool syncInput) {
@@ -339,10 +340,16 @@ std::ostream &KernelMatmul::print(std::ostream &os) const {
            << (extraParam() ? extraParam() : 4) << " K-slices\n";
     } else {
         const size_t bm = groupHeight() * blockHeight(), bn = groupWidth() * blockWidth();
-        os << "// " << (variant_ == Variant::Image ? "gemm_image_kernel" : "gemm_simt_kernel") << "<"
+        const bool img = variant_ == Variant::Image;
+        os << "// " << (img ? "gemm_image_kernel" : "gemm_simt_kernel") << "<"
            << scalar_name(scalar_) << ", TA=" << transposeA() << ", TB=" << transposeB() << ", GH=" << groupHeight()
-           << ", GW=" << groupWidth() << ", BH=" << blockHeight() << ", BW=" << blockWidth() << ", VL=" << vl_
-           << ", BK=8>\n"
+           << ", GW=" << groupWidth() << ", BH=" << blockHeight() << ", BW=" << blockWidth();
+        if (img)
+            os << ", BK=" << (scalar_ == Scalar::Double ? 16 : 32)
+               << ">: operand tiles by TMA tensor maps through a 3-stage mbarrier ring\n";
+        else
+            os << ", VL=" << vl_ << ", BK=8>\n";
+        os
            << "// thread block " << groupHeight() << "x" << groupWidth() << ", CTA tile " << bm << "x" << bn
            << ", per-thread micro-tile " << blockHeight() << "x" << blockWidth()
            << ", grid (" << (dimN() + bn - 1) / bn << ", " << (dimM() + bm - 1) / bm << ", " << packedCalc() << ")\n"
@@ -351,7 +358,7 @@ std::ostream &KernelMatmul::print(std::ostream &os) const {
         for (size_t i = 0; i < x.size(); ++i) os << (i ? " " : "") << x[i];
         os << ") [inlineMNK, loopOrder" << (variant_ == Variant::Image ? ", globalID" : "")
            << "]: recorded; every order accumulates k = 0..K-1 in sequence\n";
-        if (variant_ == Variant::Buffer) os << "\n" << jit::simt_source(jit_point());
+        os << "\n" << jit::simt_source(jit_point());
     }
     return os;
 }

@@ -152,7 +152,7 @@ static int matmul_dispatch(const gatlas_matmul_desc *d, const T *A, const T *B, 
     Geometry g;
     if (!resolve_geometry(d, &g)) return set_error(GATLAS_ERR_INVALID, "matmul: invalid dimensions or leading dimensions");
     if (g.M == 0 || g.N == 0) return GATLAS_OK;
-    if (!A || !B || !C) return set_error(GATLAS_ERR_INVALID, "matmul: null pointer");
+    if (!C || (g.K > 0 && (!A || !B))) return set_error(GATLAS_ERR_INVALID, "matmul: null pointer");
     if (g.batch > 65535) return set_error(GATLAS_ERR_INVALID, "matmul: batch > 65535");
     switch (d->engine) {
         case GATLAS_ENGINE_BUFFER: return matmul_simt<T>(d, g, A, B, C, stream);

@@ -29,6 +29,9 @@ namespace {
 const char kSimtSource[] =
 #include "gemm_simt_source.inc"
     ;
+const char kImageSource[] =
+#include "gemm_image_source.inc"
+    ;
 
 // NVRTC entry points (nvrtc.h), resolved with dlsym.
 typedef int nvrtcResult;
@@ -51,6 +54,7 @@ struct Driver {
     CUresult (*get_function)(CUfunction *, CUmodule, const char *) = nullptr;
     CUresult (*launch)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, CUstream,
                        void **, void **) = nullptr;
+    CUresult (*set_attr)(CUfunction, CUfunction_attribute, int) = nullptr;
     bool ok = false;
 };
 
@@ -58,7 +62,7 @@ std::once_flag g_once;
 Nvrtc g_nvrtc;
 Driver g_drv;
 std::mutex g_mu;
-std::map<std::tuple<int, int, int, int, int, int, int, int, int>, CUfunction> g_cache;
+std::map<std::tuple<int, int, int, int, int, int, int, int, int, int>, CUfunction> g_cache;
 
 template <typename F>
 bool sym(void *h, const char *name, F *out) {
@@ -95,7 +99,7 @@ void init() {
 bool init_driver() {
     if (g_drv.ok) return true;
     g_drv.ok = drv("cuModuleLoadData", &g_drv.load) && drv("cuModuleGetFunction", &g_drv.get_function) &&
-               drv("cuLaunchKernel", &g_drv.launch);
+               drv("cuLaunchKernel", &g_drv.launch) && drv("cuFuncSetAttribute", &g_drv.set_attr);
     return g_drv.ok;
 }
 
@@ -108,27 +112,48 @@ bool available() {
 
 std::string simt_name(const Point &p) {
     std::stringstream ss;
-    ss << "gatlas::simt::gemm_simt_kernel<" << (p.scalar ? "double" : "float") << ", " << (p.ta ? "true" : "false")
-       << ", " << (p.tb ? "true" : "false") << ", " << p.gh << ", " << p.gw << ", " << p.bh << ", " << p.bw << ", "
-       << p.vl << ", 8>";
+    const char *T = p.scalar ? "double" : "float";
+    if (p.image) {
+        ss << "gatlas::img::gemm_image_kernel<" << T << ", " << (p.ta ? "true" : "false") << ", "
+           << (p.tb ? "true" : "false") << ", " << p.gh << ", " << p.gw << ", " << p.bh << ", " << p.bw << ">";
+    } else {
+        ss << "gatlas::simt::gemm_simt_kernel<" << T << ", " << (p.ta ? "true" : "false") << ", "
+           << (p.tb ? "true" : "false") << ", " << p.gh << ", " << p.gw << ", " << p.bh << ", " << p.bw << ", "
+           << p.vl << ", 8>";
+    }
     return ss.str();
 }
 
 std::string simt_source(const Point &p) {
     std::stringstream ss;
-    ss << kSimtSource << "\n// instantiation compiled for this point:\ntemplate __global__ void " << simt_name(p)
-       << "(gatlas::simt::GemmArgs<" << (p.scalar ? "double" : "float") << ">);\n";
+    const char *T = p.scalar ? "double" : "float";
+    ss << (p.image ? kImageSource : kSimtSource) << "\n// instantiation compiled for this point:\ntemplate __global__ void "
+       << simt_name(p);
+    if (p.image)
+        ss << "(const __grid_constant__ gatlas::img::TmapBlob, const __grid_constant__ gatlas::img::TmapBlob, "
+              "gatlas::img::ImgArgs<"
+           << T << ">);\n";
+    else
+        ss << "(gatlas::simt::GemmArgs<" << T << ">);\n";
     return ss.str();
 }
 
-// Whether the template accepts the point (mirrors the static_asserts).
+// Whether the template accepts the point (mirrors the static_asserts and,
+// for the image template, the tensor-map alignment rules).
 bool point_ok(const Point &p) {
     if (p.gh < 1 || p.gw < 1 || p.bh < 1 || p.bw < 1 || p.gh * p.gw > 1024) return false;
+    if (p.bh > 16 || p.bw > 16) return false;
+    if (p.image) {
+        const int per16 = p.scalar ? 2 : 4;  // elements per 16 bytes
+        if (p.ta && (p.gh * p.bh) % per16) return false;
+        if (!p.tb && (p.gw * p.bw) % per16) return false;
+        if (p.gh * p.bh > 256 || p.gw * p.bw > 256) return false;
+        return true;
+    }
     if (p.vl != 1 && p.vl != 2 && p.vl != 4) return false;
     if (8 % p.vl != 0) return false;
     if (p.ta && (p.gh * p.bh) % p.vl != 0) return false;
     if (!p.tb && (p.gw * p.bw) % p.vl != 0) return false;
-    if (p.bh > 16 || p.bw > 16) return false;
     return true;
 }
 
@@ -137,7 +162,7 @@ int simt_function(const Point &p, void **fn) {
     if (!point_ok(p)) return set_error(GATLAS_ERR_UNSUPPORTED, "jit: the SIMT template does not take this point");
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "jit: no current device");
-    const auto key = std::make_tuple(dev, p.scalar, p.ta, p.tb, p.gh, p.gw, p.bh, p.bw, p.vl);
+    const auto key = std::make_tuple(dev, p.image, p.scalar, p.ta, p.tb, p.gh, p.gw, p.bh, p.bw, p.image ? 0 : p.vl);
     std::lock_guard<std::mutex> lk(g_mu);
     auto it = g_cache.find(key);
     if (it != g_cache.end()) {
@@ -148,7 +173,8 @@ int simt_function(const Point &p, void **fn) {
     cudaFree(nullptr);  // make the runtime's primary context current
     const Nvrtc &n = g_nvrtc;
     nvrtcProgram prog = nullptr;
-    if (n.create(&prog, kSimtSource, "gemm_simt.cu", 0, nullptr, nullptr) != 0)
+    if (n.create(&prog, p.image ? kImageSource : kSimtSource, p.image ? "gemm_image.cu" : "gemm_simt.cu", 0, nullptr,
+                 nullptr) != 0)
         return set_error(GATLAS_ERR_CUDA, "jit: nvrtcCreateProgram failed");
     const std::string name = simt_name(p);
     n.add_name(prog, name.c_str());
@@ -176,6 +202,16 @@ int simt_function(const Point &p, void **fn) {
         return set_error(GATLAS_ERR_CUDA, "jit: loading the compiled module failed");
     g_cache[key] = f;
     *fn = f;
+    return GATLAS_OK;
+}
+
+int launch_args(void *fn, unsigned gx, unsigned gy, unsigned gz, unsigned block, unsigned smem, void **args,
+                cudaStream_t stream) {
+    if (smem > 48 * 1024 &&
+        g_drv.set_attr(static_cast<CUfunction>(fn), CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem) != CUDA_SUCCESS)
+        return set_error(GATLAS_ERR_CUDA, "jit: shared memory attribute");
+    CUresult r = g_drv.launch(static_cast<CUfunction>(fn), gx, gy, gz, block, 1, 1, smem, (CUstream)stream, args, nullptr);
+    if (r != CUDA_SUCCESS) return set_error(GATLAS_ERR_CUDA, "jit: cuLaunchKernel failed (%d)", (int)r);
     return GATLAS_OK;
 }
 

@@ -11,6 +11,7 @@ namespace jit {
 struct Point {
     int scalar;  // 0 float, 1 double
     int ta, tb, gh, gw, bh, bw, vl;
+    int image = 0;  // 0: buffer template (gemm_simt.cuh), 1: image template (gemm_image.cuh)
 };
 
 bool available();                          // NVRTC loaded
@@ -21,6 +22,9 @@ std::string simt_source(const Point &p);   // full CUDA source compiled for the 
 int simt_function(const Point &p, void **fn);
 // Launch a compiled kernel with one by-value argument block.
 int launch(void *fn, unsigned gx, unsigned gy, unsigned gz, unsigned block, void *args, cudaStream_t stream);
+// Launch with several by-value arguments and dynamic shared memory.
+int launch_args(void *fn, unsigned gx, unsigned gy, unsigned gz, unsigned block, unsigned smem, void **args,
+                cudaStream_t stream);
 
 }  // namespace jit
 }  // namespace gatlas

@@ -143,3 +143,76 @@ def test_full_size_residual_4096(cuda):
     Ah = A.view(M, K)[rows].cpu().numpy().ravel()
     ref_rows = oracle.matmul(Ah, B.cpu().numpy(), len(rows), N, K, mode=oracle.FMA)
     assert np.array_equal(C.view(M, N)[rows].cpu().numpy().ravel(), ref_rows)
+
+
+# ---- image engine: SIMT math on TMA tensor-map tiles ------------------------------
+
+IMAGE_TILES = [(16, 16, 8, 8), (16, 16, 8, 4), (8, 8, 8, 4), (16, 16, 4, 4), (8, 8, 4, 4)]
+
+
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("tile", IMAGE_TILES, ids=lambda t: "x".join(map(str, t)))
+def test_image_engine_bit_exact(cuda, ta, tb, tile):
+    M, N, K = 256, 192, 100
+    A = oracle.uniform(M * K, seed=sum(tile) + ta)
+    B = oracle.uniform(K * N, seed=sum(tile) + 7 * tb)
+    C = _mm(cuda, A, B, M, N, K, ta, tb, tile=tile + (0,), engine="image")
+    assert np.array_equal(C, oracle.matmul(A, B, M, N, K, ta, tb, mode=oracle.FMA))
+    assert g.device_faults() == 0
+
+
+@pytest.mark.parametrize("ta,tb", [(0, 0), (1, 1)])
+@pytest.mark.parametrize("M,N,K", [(4, 4, 4), (36, 68, 33), (130, 260, 64), (3520 // 10, 3520 // 10, 3520 // 10)])
+def test_image_engine_ragged(cuda, ta, tb, M, N, K):
+    # rows need 16-byte alignment for TMA: the stored inner dimensions are multiples of 4 here
+    if (K if not ta else M) % 4 or (N if not tb else K) % 4:
+        pytest.skip("TMA needs 16-byte aligned rows")
+    A = oracle.uniform(M * K, seed=M)
+    B = oracle.uniform(K * N, seed=N)
+    C = _mm(cuda, A, B, M, N, K, ta, tb, engine="image")
+    assert np.array_equal(C, oracle.matmul(A, B, M, N, K, ta, tb, mode=oracle.FMA))
+
+
+def test_image_engine_gemm_batch_and_known_answer(cuda):
+    M, N, K, P = 128, 128, 96, 2
+    A = oracle.uniform(P * M * K, seed=3)
+    B = oracle.uniform(P * K * N, seed=4)
+    Cin = oracle.uniform(P * M * N, seed=5)
+    C = _mm(cuda, A, B, M, N, K, gemm=True, Cin=Cin, alpha=0.5, beta=2.0, batch=P, engine="image")
+    assert np.array_equal(C, oracle.matmul(A, B, M, N, K, mode=oracle.FMA, gemm=1, Cin=Cin, alpha=0.5, beta=2.0,
+                                           packed=P))
+    C = _mm(cuda, np.ones(512 * 512, np.float32), np.ones(512 * 512, np.float32), 512, 512, 512, engine="image")
+    assert oracle.check_pattern(C, 512.0)
+
+
+@pytest.mark.parametrize("tile", [(16, 16, 12, 4), (9, 9, 4, 4), (10, 10, 8, 4)])
+def test_image_engine_run_time_compiled(cuda, tile):
+    gh, gw, bh, bw = tile
+    M, N, K = gh * bh * 2, gw * bw * 2, 64
+    A = oracle.uniform(M * K, seed=11)
+    B = oracle.uniform(K * N, seed=12)
+    C = _mm(cuda, A, B, M, N, K, tile=tile + (0,), engine="image")
+    assert np.array_equal(C, oracle.matmul(A, B, M, N, K, mode=oracle.FMA))
+
+
+@pytest.mark.parametrize("ta,tb", [(0, 0), (1, 0)])
+def test_image_engine_double(cuda, ta, tb):
+    M, N, K = 128, 96, 80
+    A = oracle.uniform(M * K, seed=8, dtype=np.float64)
+    B = oracle.uniform(K * N, seed=9, dtype=np.float64)
+    C = _mm(cuda, A, B, M, N, K, ta, tb, engine="image")
+    assert np.array_equal(C, oracle.matmul(A, B, M, N, K, ta, tb, mode=oracle.FMA, dtype=np.float64))
+
+
+def test_image_engine_empty_contraction_and_unaligned_rows(cuda):
+    M, N = 64, 64
+    Cin = oracle.uniform(M * N, seed=21)
+    C = _mm(cuda, np.zeros(0, np.float32), np.zeros(0, np.float32), M, N, 0, gemm=True, Cin=Cin, alpha=1.0,
+            beta=0.5, engine="image")
+    assert np.array_equal(C, oracle.matmul(np.zeros(0, np.float32), np.zeros(0, np.float32), M, N, 0, mode=oracle.FMA,
+                                           gemm=1, Cin=Cin, alpha=1.0, beta=0.5))
+    # K = 30 gives A rows of 120 bytes: TMA needs 16-byte aligned rows, the engine refuses
+    A = oracle.uniform(M * 30, seed=1)
+    B = oracle.uniform(30 * N, seed=2)
+    with pytest.raises(RuntimeError, match="16-byte"):
+        _mm(cuda, A, B, M, N, 30, engine="image")

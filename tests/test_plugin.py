@@ -118,3 +118,48 @@ def test_print_describes_the_cuda_instance():
     text = k.print()
     assert "gemm_simt_kernel<float" in text and "GH=16" in text and "BH=8" in text
     assert "extra parameter 3 = (1 1)" in text
+    assert "template __global__ void gatlas::simt::gemm_simt_kernel<float, false, false, 16, 16, 8, 4, 4, 8>" in text
+
+
+def test_print_image_instance_carries_image_source():
+    k = Kernel("matmul", "floatimg")
+    k.set_params([1, 0, 1024, 1024, 1024, 1, 0, 16, 16, 8, 4, 0])
+    text = k.print()
+    assert "gemm_image_kernel<float, TA=1, TB=0" in text and "BK=32" in text
+    assert "template __global__ void gatlas::img::gemm_image_kernel<float, true, false, 16, 16, 8, 4>" in text
+
+
+def _nvrtc_compile(src):
+    """Compiles src for sm_100a with NVRTC (no GPU needed); returns (status, log)."""
+    import ctypes
+    try:
+        nv = ctypes.CDLL("libnvrtc.so.12")
+    except OSError:
+        pytest.skip("NVRTC is not installed")
+    prog = ctypes.c_void_p()
+    assert nv.nvrtcCreateProgram(ctypes.byref(prog), src.encode(), b"point.cu", 0, None, None) == 0
+    opts = [b"--gpu-architecture=sm_100a", b"-std=c++17", b"-default-device", b"-lineinfo"]
+    rc = nv.nvrtcCompileProgram(prog, len(opts), (ctypes.c_char_p * len(opts))(*opts))
+    n = ctypes.c_size_t()
+    nv.nvrtcGetProgramLogSize(prog, ctypes.byref(n))
+    log = ctypes.create_string_buffer(n.value)
+    nv.nvrtcGetProgramLog(prog, log)
+    nv.nvrtcDestroyProgram(ctypes.byref(prog))
+    return rc, log.value.decode(errors="replace")
+
+
+@pytest.mark.parametrize("t,p", [
+    ("float4", [1, 0, 640, 640, 640, 1, 0, 10, 10, 8, 4, 0]),
+    ("double1", [1, 1, 640, 640, 640, 0, 1, 8, 8, 10, 1, 2]),
+    ("floatimg", [1, 0, 640, 640, 640, 0, 1, 10, 10, 8, 4, 0]),
+    ("floatimg", [1, 0, 768, 768, 768, 0, 0, 16, 16, 12, 4, 0]),
+    ("doubleimg", [1, 0, 648, 648, 648, 1, 0, 9, 9, 4, 4, 0]),
+])
+def test_run_time_compiled_source_compiles(t, p):
+    # the source print() shows is exactly what run-time compilation builds
+    k = Kernel("matmul", t)
+    k.set_params(p)
+    text = k.print()
+    src = text[text.index("\n\n") + 2:]
+    rc, log = _nvrtc_compile(src)
+    assert rc == 0, log
