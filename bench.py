@@ -157,6 +157,7 @@ def _max_over_ranks(x: float, world: int) -> float:
 
 HEADLINE_ENGINE = "tc_split3"     # FP32 operands as BF16 hi/lo, 3 products, FP32 accumulation
 PRODUCTS = {"tc_bf16": 1, "tc_split3": 3, "tc_split6": 6}
+SWEEP_ENGINES = ("buffer", "tc_bf16", "tc_split3", "tc_split6", "tc_fp8")
 
 
 def _timed(fn, steps, warmup, world, stream):
@@ -201,7 +202,7 @@ def run_ours(args, rank, world, local):
     C = torch.empty(M * N, dtype=torch.float32, device=dev)
     g.fill(A, "uniform", seed=1 + rank)
     g.fill(B, "uniform", seed=2 + rank)
-    ws_bytes = max(g.matmul_workspace_size(M, N, K, e) for e in PRODUCTS)
+    ws_bytes = max(g.matmul_workspace_size(M, N, K, e) for e in SWEEP_ENGINES if e != "buffer")
     ws = torch.empty(ws_bytes + 1024, dtype=torch.uint8, device=dev)
     ws = ws[(-ws.data_ptr()) % 1024:][:ws_bytes]          # 1024-byte aligned view
     step = _gemm_step_fn(g, A, B, C, M, N, K, engine, ws if engine != "buffer" else None)
@@ -260,12 +261,21 @@ def run_ours(args, rank, world, local):
         for dist in ("uniform", "pow2"):
             g.fill(A, dist, seed=11)
             g.fill(B, dist, seed=12)
-            for eng in ("buffer", "tc_bf16", "tc_split3", "tc_split6"):
+            for eng in SWEEP_ENGINES:
+                if not g.matmul_supported(eng):
+                    continue
                 f = _gemm_step_fn(g, A, B, C, M, N, K, eng, ws if eng != "buffer" else None)
                 t = _timed(f, 3 if eng == "buffer" else 5, 1, world, stream)
                 fr, rn, mxe, _ = g.residual(A, B, C, M, N, K)
-                sweep[f"{eng}_{dist}"] = {"tflops": flops / (t * 1e-3) / 1e12, "ms": t,
-                                          "normwise_err": fr / rn, "max_abs_err": mxe}
+                row = {"tflops": flops / (t * 1e-3) / 1e12, "ms": t, "normwise_err": fr / rn,
+                       "max_abs_err": mxe}
+                if eng != "buffer":
+                    # the contraction alone on operands prepared once
+                    g.matmul_tc_prepare(A, B, M, N, K, ws, engine=eng)
+                    tk = _timed(lambda: g.matmul_tc_run(ws, M, N, K, C, engine=eng), 5, 1, world, stream)
+                    row["kernel_ms"] = tk
+                    row["kernel_tflops"] = flops / (tk * 1e-3) / 1e12
+                sweep[f"{eng}_{dist}"] = row
         Md = 4096
         Ad = torch.empty(Md * Md, dtype=torch.float64, device=dev)
         Bd = torch.empty(Md * Md, dtype=torch.float64, device=dev)
@@ -406,7 +416,7 @@ def run_reference(args, rank, world):
 
 def run_case(spec: str) -> None:
     """Small single-kernel cases for ncu captures: NAME:SIZE, three calls each.
-    tc_bf16|tc_split3|tc_split6:M (M^3 GEMM, prepare once, run x3), sgemm_simt:M,
+    tc_bf16|tc_split3|tc_split6|tc_fp8:M (M^3 GEMM, prepare once, run x3), sgemm_simt:M,
     gemv_A:N / gemv_At:N (N^2 GEMV), saxpy_buffer:n / saxpy_image:n."""
     import torch
 

@@ -3,7 +3,7 @@
 // Reference: benchMatmul.cpp (options :68-215, search :217-304, main loop
 // :307-405, brute force :498-534, EM :536-627, final average :630-650).
 // Same options and output lines; -d gpuN selects a CUDA device; -T also takes
-// the tensor-core types tcbf16, split3 and split6.  When the device cannot be
+// the tensor-core types tcbf16, split3, split6 and fp8.  When the device cannot be
 // opened the tool still replays a search whose every point is already in the
 // journal.
 #include <unistd.h>
@@ -42,7 +42,7 @@ bool parse(int argc, char **argv, Opts &o) {
             case 'h':
                 cerr << "usage: " << argv[0]
                      << " -d gpu|gpuX -j journalFile -T float1|float2|float4|double1|double2|double4|floatimg|doubleimg"
-                        "|tcbf16|split3|split6 -n N [-m M -k K] [-C numKernels] [-g groupSize [-y blockHeight"
+                        "|tcbf16|split3|split6|fp8 -n N [-m M -k K] [-C numKernels] [-g groupSize [-y blockHeight"
                         " [-x extraParam]]] [-t numberTrials] [-w topN] [-G] [-e] [-a] [-b] [-s] [-r] [-p] [-v] [-z] [-h]"
                      << endl
                      << "\t-d gpu device, optional X is the CUDA device number" << endl

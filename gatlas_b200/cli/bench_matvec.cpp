@@ -75,7 +75,7 @@ bool parse(int argc, char **argv, Opts &o) {
     Scalar s;
     Variant v;
     if (!parse_type(o.type, &s, &v, &o.vl) || v == Variant::TcBf16 || v == Variant::TcSplit3 ||
-        v == Variant::TcSplit6) {
+        v == Variant::TcSplit6 || v == Variant::TcFp8) {
         cerr << "error: invalid kernel type of " << o.type << endl;
         rc = false;
         o.vl = 1;

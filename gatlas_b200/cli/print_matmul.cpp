@@ -28,7 +28,7 @@ int main(int argc, char **argv) {
         switch (opt) {
             case 'h':
                 cerr << "usage: " << argv[0]
-                     << " -T float1|float2|float4|double1|double2|double4|floatimg|doubleimg|tcbf16|split3|split6"
+                     << " -T float1|float2|float4|double1|double2|double4|floatimg|doubleimg|tcbf16|split3|split6|fp8"
                         " -n N [-m M -k K] -g groupSize -y blockHeight -x extraParam [-C numKernels] [-G] [-a] [-b]"
                         " [-v] [-h]"
                      << endl;

@@ -113,12 +113,13 @@ static int engine_of(Variant v) {
         case Variant::TcBf16: return GATLAS_ENGINE_TC_BF16;
         case Variant::TcSplit3: return GATLAS_ENGINE_TC_SPLIT3;
         case Variant::TcSplit6: return GATLAS_ENGINE_TC_SPLIT6;
+        case Variant::TcFp8: return GATLAS_ENGINE_TC_FP8;
     }
     return -1;
 }
 
 static bool is_tc(Variant v) {
-    return v == Variant::TcBf16 || v == Variant::TcSplit3 || v == Variant::TcSplit6;
+    return v == Variant::TcBf16 || v == Variant::TcSplit3 || v == Variant::TcSplit6 || v == Variant::TcFp8;
 }
 
 // Normwise error budgets of the tensor-core engines against FP64.
@@ -126,6 +127,7 @@ static double tc_budget(Variant v) {
     switch (v) {
         case Variant::TcBf16: return std::ldexp(1.0, -7);
         case Variant::TcSplit3: return 8e-6;
+        case Variant::TcFp8: return std::ldexp(1.0, -4);  // E4M3 unit roundoff per operand
         default: return 2.5e-6;
     }
 }
@@ -333,7 +335,12 @@ std::ostream &KernelMatmul::print(std::ostream &os) const {
     os << "// " << kernelName() << "  M=" << dimM() << " N=" << dimN() << " K=" << dimK()
        << " transposeA=" << transposeA() << " transposeB=" << transposeB()
        << " GEMM=" << generalizedMatmul() << " packed=" << packedCalc() << "\n";
-    if (is_tc(variant_)) {
+    if (variant_ == Variant::TcFp8) {
+        os << "// quant_fp8_kernel: E4M3 codes with one power-of-two FP32 scale per 128x128 block\n"
+           << "// tcgen05 kernel tc_gemm_kernel<tcfp8>: 128x256 output tile per CTA, TMA 128B-swizzled E4M3 tiles "
+           << "(BK=128), tcgen05.mma kind::f8f6f4 M=128 N=256 K=32, each 128-deep block scaled and promoted into "
+           << "FP32 registers\n";
+    } else if (is_tc(variant_)) {
         os << "// tcgen05 kernel tc_gemm_kernel<" << variant_name(variant_)
            << ">: 128x256 output tile per CTA, TMA 64B-swizzled BF16 piece tiles (BK=32), "
            << "tcgen05.mma kind::f16 M=128 N=256 K=16, FP32 accumulation in TMEM promoted every "
@@ -634,6 +641,7 @@ bool parse_type(const std::string &t, Scalar *s, Variant *v, size_t *vl) {
         {"floatimg", Scalar::Float, Variant::Image, 4},  {"doubleimg", Scalar::Double, Variant::Image, 2},
         {"tcbf16", Scalar::Float, Variant::TcBf16, 4},   {"split3", Scalar::Float, Variant::TcSplit3, 4},
         {"split6", Scalar::Float, Variant::TcSplit6, 4},
+        {"fp8", Scalar::Float, Variant::TcFp8, 4},
     };
     for (const Row &r : rows)
         if (t == r.name) {

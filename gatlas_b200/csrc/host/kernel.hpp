@@ -174,7 +174,7 @@ class KernelSaxpy : public KernelInterface, public SaxpyParams {
 };
 
 // Factory from the reference's -T kernel type names (benchMatmul.cpp:141-160),
-// extended with the tensor-core types tcbf16, split3 and split6 (matmul only).
+// extended with the tensor-core types tcbf16, split3, split6 and fp8 (matmul only).
 // op: "matmul" | "matvec" | "saxpy".  Returns nullptr for unknown types.
 KernelInterface *make_kernel(const std::string &op, const std::string &type);
 

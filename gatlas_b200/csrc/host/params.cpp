@@ -24,6 +24,7 @@ const char *variant_name(Variant v) {
         case Variant::TcBf16: return "tcbf16";
         case Variant::TcSplit3: return "tcsplit3";
         case Variant::TcSplit6: return "tcsplit6";
+        case Variant::TcFp8: return "tcfp8";
     }
     return "?";
 }

@@ -37,7 +37,7 @@ class ExtraParameter {
 };
 
 enum class Scalar { Float, Double };
-enum class Variant { Buffer, Image, TcBf16, TcSplit3, TcSplit6 };
+enum class Variant { Buffer, Image, TcBf16, TcSplit3, TcSplit6, TcFp8 };
 
 const char *scalar_name(Scalar s);
 const char *variant_name(Variant v);

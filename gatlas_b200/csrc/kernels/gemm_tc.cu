@@ -24,6 +24,7 @@
 // fault word, stops the pipeline, drains the copies in flight and frees TMEM.
 #include <cuda.h>
 #include <cuda_bf16.h>
+#include <cuda_fp8.h>
 
 #include "../common.cuh"
 #include "../device_state.cuh"
@@ -34,59 +35,81 @@
 namespace gatlas {
 namespace tcg {
 
-constexpr int BM = 128, BN = 256, BK = 32;
+constexpr int BM = 128, BN = 256;
 constexpr int kGroupM = 16;  // tile rows per raster group
 
-// Default promotion interval: 4 slices of BK = 32, i.e. K = 128 per
-// TMEM segment (selectable per call through the descriptor's extra field).
+// Default promotion interval for the BF16 modes: 4 slices of 32, i.e.
+// K = 128 per TMEM segment (selectable per call through the descriptor's
+// extra field).  The FP8 mode promotes every slice (one scale block).
 constexpr int kDefaultSegKblocks = 4;
-constexpr uint32_t kRowBytes = BK * 2;        // 64 B rows -> 64-byte swizzle
-constexpr uint32_t kSBO = 8 * kRowBytes;      // 8-row core-matrix groups
-constexpr uint32_t kATile = BM * kRowBytes;   // 8 KiB
-constexpr uint32_t kBTile = BN * kRowBytes;   // 16 KiB
-constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s bound on any single wait
+constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s bound on any single wait
 
 // MODE 0: one BF16 piece, one product; 1: two pieces, three products;
-// 2: three pieces, six products.
+// 2: three pieces, six products; 3: FP8 E4M3 codes with one FP32 scale per
+// 128 x 128 block of each operand.  Every mode stages K slices of 32 bytes
+// per MMA instruction: K = 16 BF16 or K = 32 E4M3 elements.
 template <int MODE>
 struct Mode;
 template <>
 struct Mode<0> {
-    static constexpr int NP = 1, NPROD = 1, STAGES = 8;
+    static constexpr int NP = 1, NPROD = 1, STAGES = 8, ELEM = 2, BKE = 32;
+    static constexpr bool SCALED = false;
     __device__ static constexpr int pa(int) { return 0; }
     __device__ static constexpr int pb(int) { return 0; }
 };
 template <>
 struct Mode<1> {
-    static constexpr int NP = 2, NPROD = 3, STAGES = 4;
+    static constexpr int NP = 2, NPROD = 3, STAGES = 4, ELEM = 2, BKE = 32;
+    static constexpr bool SCALED = false;
     // hi*hi, hi*lo, lo*hi
     __device__ static constexpr int pa(int j) { return j == 2 ? 1 : 0; }
     __device__ static constexpr int pb(int j) { return j == 1 ? 1 : 0; }
 };
 template <>
 struct Mode<2> {
-    static constexpr int NP = 3, NPROD = 6, STAGES = 3;
+    static constexpr int NP = 3, NPROD = 6, STAGES = 3, ELEM = 2, BKE = 32;
+    static constexpr bool SCALED = false;
     // hi*hi, hi*mid, mid*hi, mid*mid, hi*lo, lo*hi
     __device__ static constexpr int pa(int j) { return j == 2 || j == 3 ? 1 : (j == 5 ? 2 : 0); }
     __device__ static constexpr int pb(int j) { return j == 1 || j == 3 ? 1 : (j == 4 ? 2 : 0); }
 };
+template <>
+struct Mode<3> {
+    static constexpr int NP = 1, NPROD = 1, STAGES = 4, ELEM = 1, BKE = 128;
+    static constexpr bool SCALED = true;
+    __device__ static constexpr int pa(int) { return 0; }
+    __device__ static constexpr int pb(int) { return 0; }
+};
 
 template <int MODE>
 struct Layout {
-    static constexpr int NP = Mode<MODE>::NP;
-    static constexpr int STAGES = Mode<MODE>::STAGES;
-    static constexpr uint32_t STAGE_BYTES = NP * (kATile + kBTile);
+    using MD = Mode<MODE>;
+    static constexpr int NP = MD::NP;
+    static constexpr int STAGES = MD::STAGES;
+    static constexpr int BK = MD::BKE;                              // elements per K slice
+    static constexpr uint32_t ROW_BYTES = BK * MD::ELEM;            // 64 (BF16) or 128 (FP8)
+    static constexpr uint32_t SWIZZLE = ROW_BYTES == 128 ? tc::kSwizzle128B : tc::kSwizzle64B;
+    static constexpr uint32_t SBO = 8 * ROW_BYTES;                  // 8-row core-matrix groups
+    static constexpr uint32_t A_TILE = BM * ROW_BYTES;
+    static constexpr uint32_t B_TILE = BN * ROW_BYTES;
+    static constexpr int KSTEPS = ROW_BYTES / 32;                   // MMA instructions per slice
+    static constexpr uint32_t STAGE_BYTES = NP * (A_TILE + B_TILE);
     static constexpr uint32_t SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + alignment slack
+    static constexpr uint32_t IDESC = MD::SCALED ? tc::idesc_e4m3_f32(BM, BN) : tc::idesc_bf16_f32(BM, BN);
 };
 
 struct Params {
     float *C;
     int64_t M, N, ldc, stride_c;
     int kblocks;
-    int seg_kblocks;  // K slices (of BK) accumulated in TMEM before promotion
+    int seg_kblocks;  // K slices accumulated in TMEM before promotion
     float alpha, beta;
     int gemm;
     int *fault;
+    // FP8 only: block scales [batch][row blocks][kblocks] of A and of B
+    const float *scale_a, *scale_b;
+    int64_t scale_a_stride, scale_b_stride;  // per instance
+    int nblocks_n;                           // 128-column blocks of N
 };
 
 // Warp roles: warp 0 = TMA producer (lane 0), warp 1 = MMA issuer (lane 0),
@@ -128,6 +151,7 @@ __global__ void __launch_bounds__(kThreads2, 1)
         tile_n = r / gm;
     }
     const int m0 = tile_m * BM, n0 = tile_n * BN, z = blockIdx.z;
+    constexpr int BK = L::BK;
     const CUtensorMap *tA[3] = {&ta0, &ta1, &ta2};
     const CUtensorMap *tB[3] = {&tb0, &tb1, &tb2};
     const int nseg = (p.kblocks + p.seg_kblocks - 1) / p.seg_kblocks;
@@ -159,8 +183,8 @@ __global__ void __launch_bounds__(kThreads2, 1)
     tc::fence_after_sync();
     const uint32_t tmem = tmem_base;
 
-    auto a_tile = [&](int s, int piece) { return smem + s * L::STAGE_BYTES + piece * kATile; };
-    auto b_tile = [&](int s, int piece) { return smem + s * L::STAGE_BYTES + MD::NP * kATile + piece * kBTile; };
+    auto a_tile = [&](int s, int piece) { return smem + s * L::STAGE_BYTES + piece * L::A_TILE; };
+    auto b_tile = [&](int s, int piece) { return smem + s * L::STAGE_BYTES + MD::NP * L::A_TILE + piece * L::B_TILE; };
 
     if (warp == 0) {
         if (lane == 0) {
@@ -186,7 +210,7 @@ __global__ void __launch_bounds__(kThreads2, 1)
     } else if (warp == 1) {
         if (lane == 0) {
             // ---- MMA issuer: segment g accumulates into TMEM buffer g & 1 ----
-            constexpr uint32_t idesc = tc::idesc_bf16_f32(BM, BN);
+            constexpr uint32_t idesc = L::IDESC;
             int kb = 0;
             for (; kb < p.kblocks; ++kb) {
                 const int seg = kb / p.seg_kblocks, b = seg & 1;
@@ -211,14 +235,17 @@ __global__ void __launch_bounds__(kThreads2, 1)
                 tc::fence_after_sync();
                 const uint32_t d = tmem + (uint32_t)(b * BN);
 #pragma unroll
-                for (int kk = 0; kk < BK / 16; ++kk) {
+                for (int kk = 0; kk < L::KSTEPS; ++kk) {
 #pragma unroll
                     for (int j = 0; j < MD::NPROD; ++j) {
+                        // 32 bytes of K per instruction inside the swizzled rows
                         const uint32_t a_addr = smem_u32(a_tile(s, MD::pa(j))) + kk * 32;
                         const uint32_t b_addr = smem_u32(b_tile(s, MD::pb(j))) + kk * 32;
-                        tc::mma_bf16(d, tc::smem_desc_kmajor(a_addr, kSBO, tc::kSwizzle64B),
-                                     tc::smem_desc_kmajor(b_addr, kSBO, tc::kSwizzle64B), idesc,
-                                     (seg_first && kk == 0 && j == 0) ? 0u : 1u);
+                        const uint64_t ad = tc::smem_desc_kmajor(a_addr, L::SBO, L::SWIZZLE);
+                        const uint64_t bd = tc::smem_desc_kmajor(b_addr, L::SBO, L::SWIZZLE);
+                        const uint32_t accum = (seg_first && kk == 0 && j == 0) ? 0u : 1u;
+                        if constexpr (MD::SCALED) tc::mma_f8(d, ad, bd, idesc, accum);
+                        else tc::mma_bf16(d, ad, bd, idesc, accum);
                     }
                 }
                 tc::commit_to(&empty[s]);
@@ -239,8 +266,19 @@ __global__ void __launch_bounds__(kThreads2, 1)
 #pragma unroll
         for (int j = 0; j < BN / 2; ++j) acc[j] = 0.0f;
         bool ok = true;
+        // FP8: this warp's column half is one 128-column scale block of B
+        const int nblk = tile_n * 2 + half;
+        const float *sa_row = MD::SCALED ? p.scale_a + z * p.scale_a_stride + (int64_t)tile_m * p.kblocks : nullptr;
+        const float *sb_row = (MD::SCALED && nblk < p.nblocks_n)
+                                  ? p.scale_b + z * p.scale_b_stride + (int64_t)nblk * p.kblocks
+                                  : nullptr;
         for (int seg = 0; seg < nseg; ++seg) {
             const int b = seg & 1;
+            float scale = 1.0f;
+            if constexpr (MD::SCALED) {
+                // loaded before the wait, so the latency hides behind it
+                scale = sb_row ? __fmul_rn(__ldg(sa_row + seg), __ldg(sb_row + seg)) : 0.0f;
+            }
             if (!tc::wait_timed(&tfull[b], (uint32_t)(seg >> 1) & 1u, 2 * kWaitNs, &abort_flag)) {
                 if (!abort_flag) report_fault(p.fault, kFaultTcEpilogueWait);
                 abort_flag = 1;
@@ -254,7 +292,12 @@ __global__ void __launch_bounds__(kThreads2, 1)
                 tc::tmem_ld_32x32b_x32(tmem + lane_base + (uint32_t)(b * BN + half * (BN / 2) + c * 32), r);
                 tc::tmem_ld_wait();
 #pragma unroll
-                for (int j = 0; j < 32; ++j) acc[c * 32 + j] = __fadd_rn(acc[c * 32 + j], __uint_as_float(r[j]));
+                for (int j = 0; j < 32; ++j) {
+                    if constexpr (MD::SCALED)
+                        acc[c * 32 + j] = __fmaf_rn(__uint_as_float(r[j]), scale, acc[c * 32 + j]);
+                    else
+                        acc[c * 32 + j] = __fadd_rn(acc[c * 32 + j], __uint_as_float(r[j]));
+                }
             }
             tc::fence_before_sync();
             __syncwarp();
@@ -383,29 +426,189 @@ __global__ void __launch_bounds__(256) split_transpose_kernel(SplitArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// FP8 pass: FP32 -> E4M3 codes, K-major [batch][rows][Kp], with one FP32
+// scale per 128 x 128 block: s = the smallest power of two with
+// amax / s <= 448, code = e4m3_rn_satfinite(x / s) (x / s is exact; all
+// codes 0 and s = 0 for an all-zero block).  Power-of-two scales keep the
+// scaling, the scale product sa * sb and the dequantisation exact.
+// ---------------------------------------------------------------------------
+constexpr int kQBlock = 128;
+
+struct QuantArgs {
+    const float *src;
+    int64_t rows, K, Kp, ld, src_stride;
+    int transposed;   // element (r,k) at src[k*ld + r] instead of src[r*ld + k]
+    int vec;          // 16-byte loads allowed: ld and src_stride multiples of 4, base 16-byte aligned
+    uint8_t *codes;   // [batch][rows][Kp]
+    float *scales;    // [batch][rblocks][kblocks]
+    int64_t rblocks, kblocks;
+};
+
+// Staged code words: row r (0..127) holds 32 words of 4 codes; word w is
+// stored at w ^ (r >> 2) so that both the staging stores (a warp covers 32
+// words of one row, or one word of 32 row quads) and the row-wise copy-out
+// hit 32 distinct banks.
+__device__ __forceinline__ int qt_index(int r, int w) { return r * 32 + (w ^ ((r >> 2) & 31)); }
+
+__device__ __forceinline__ uint32_t e4m3_pack4(float s, float x0, float x1, float x2, float x3) {
+    if (s == 0.0f) return 0u;
+    const uint32_t b0 = __nv_cvt_float_to_fp8(__fdiv_rn(x0, s), __NV_SATFINITE, __NV_E4M3);
+    const uint32_t b1 = __nv_cvt_float_to_fp8(__fdiv_rn(x1, s), __NV_SATFINITE, __NV_E4M3);
+    const uint32_t b2 = __nv_cvt_float_to_fp8(__fdiv_rn(x2, s), __NV_SATFINITE, __NV_E4M3);
+    const uint32_t b3 = __nv_cvt_float_to_fp8(__fdiv_rn(x3, s), __NV_SATFINITE, __NV_E4M3);
+    return b0 | (b1 << 8) | (b2 << 16) | (b3 << 24);
+}
+
+__global__ void __launch_bounds__(256) quant_fp8_kernel(QuantArgs a) {
+    __shared__ uint32_t qt[kQBlock * 32];
+    __shared__ float red[8];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int64_t r0 = (int64_t)blockIdx.y * kQBlock, k0 = (int64_t)blockIdx.x * kQBlock, z = blockIdx.z;
+    const float *src = a.src + z * a.src_stride;
+    // 64 values per thread as 16 groups of 4 consecutive elements of the
+    // stored inner dimension (k for direct sources, rows for transposed ones)
+    float v[64];
+    float amax = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        int64_t outer, inner;  // stored coordinates of the group's first element
+        if (!a.transposed) {
+            const int idx = i * 256 + tid;                  // row idx/32, k quad idx%32
+            outer = r0 + (idx >> 5);
+            inner = k0 + (idx & 31) * 4;
+        } else {
+            const int blk = (i >> 2) * 256 + tid;           // 4x4 block: row quad blk%32, k quad blk/32
+            outer = k0 + (blk >> 5) * 4 + (i & 3);
+            inner = r0 + (blk & 31) * 4;
+        }
+        const int64_t outer_lim = a.transposed ? a.K : a.rows, inner_lim = a.transposed ? a.rows : a.K;
+        float x[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        if (outer < outer_lim) {
+            const float *ptr = src + outer * a.ld + inner;
+            if (a.vec && inner + 3 < inner_lim) {
+                const float4 q = __ldg(reinterpret_cast<const float4 *>(ptr));
+                x[0] = q.x, x[1] = q.y, x[2] = q.z, x[3] = q.w;
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                    if (inner + e < inner_lim) x[e] = ptr[e];
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            v[i * 4 + e] = x[e];
+            amax = fmaxf(amax, fabsf(x[e]));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    if (lane == 0) red[warp] = amax;
+    __syncthreads();
+    amax = red[0];
+#pragma unroll
+    for (int w = 1; w < 8; ++w) amax = fmaxf(amax, red[w]);
+    // s = 2^ceil(log2(amax / 448)), the smallest power of two with amax / s <= 448:
+    // with amax = f * 2^e, f in [0.5, 1), that is 2^(e - 9) for f <= 0.875, else 2^(e - 8)
+    float s = 0.0f;
+    if (amax > 0.0f) {
+        int e;
+        const float f = frexpf(amax, &e);
+        s = ldexpf(1.0f, e - 9 + (f > 0.875f ? 1 : 0));
+    }
+    if (tid == 0) a.scales[(z * a.rblocks + blockIdx.y) * a.kblocks + blockIdx.x] = s;
+    if (!a.transposed) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const int idx = i * 256 + tid;
+            qt[qt_index(idx >> 5, idx & 31)] = e4m3_pack4(s, v[i * 4], v[i * 4 + 1], v[i * 4 + 2], v[i * 4 + 3]);
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int blk = j * 256 + tid;
+            const int rq = blk & 31, kq = blk >> 5;
+            // v[(j*4 + kk)*4 + e] is element (row 4*rq + e, k 4*kq + kk)
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                qt[qt_index(rq * 4 + e, kq)] = e4m3_pack4(s, v[(j * 4 + 0) * 4 + e], v[(j * 4 + 1) * 4 + e],
+                                                          v[(j * 4 + 2) * 4 + e], v[(j * 4 + 3) * 4 + e]);
+        }
+    }
+    __syncthreads();
+    uint8_t *codes = a.codes + z * a.rows * a.Kp;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int idx = i * 256 + tid;
+        const int r = idx >> 5, w = idx & 31;
+        const int64_t row = r0 + r, k = k0 + w * 4;
+        if (row < a.rows && k < a.Kp)
+            *reinterpret_cast<uint32_t *>(codes + row * a.Kp + k) = qt[qt_index(r, w)];
+    }
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 struct Plan {
-    int mode;  // 0 bf16, 1 split3, 2 split6
-    int np;
+    int mode;  // 0 bf16, 1 split3, 2 split6, 3 fp8
+    int np;    // operand pieces
+    int elem;  // bytes per staged element
     int64_t Kp;
-    size_t a_piece_bytes, b_piece_bytes, total;
+    size_t a_piece_bytes, b_piece_bytes;
+    // FP8: scale blocks
+    int64_t mblocks, nblocks, kblocks;
+    size_t sa_bytes, sb_bytes;
+    size_t total;
 };
 
 static inline size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 static bool make_plan(const gatlas_matmul_desc *d, const Geometry &g, Plan *pl) {
+    pl->elem = 2;
     switch (d->engine) {
         case GATLAS_ENGINE_TC_BF16: pl->mode = 0; pl->np = 1; break;
         case GATLAS_ENGINE_TC_SPLIT3: pl->mode = 1; pl->np = 2; break;
         case GATLAS_ENGINE_TC_SPLIT6: pl->mode = 2; pl->np = 3; break;
+        case GATLAS_ENGINE_TC_FP8: pl->mode = 3; pl->np = 1; pl->elem = 1; break;
         default: return false;
     }
-    pl->Kp = (int64_t)round_up((size_t)(g.K > 0 ? g.K : 1), 8);
-    pl->a_piece_bytes = round_up((size_t)g.batch * (size_t)g.M * (size_t)pl->Kp * 2, 1024);
-    pl->b_piece_bytes = round_up((size_t)g.batch * (size_t)g.N * (size_t)pl->Kp * 2, 1024);
-    pl->total = pl->np * (pl->a_piece_bytes + pl->b_piece_bytes);
+    const size_t K = (size_t)(g.K > 0 ? g.K : 1);
+    // rows of 16 bytes at least (TMA row pitch), zero padded to Kp
+    pl->Kp = (int64_t)round_up(K, 16 / pl->elem);
+    pl->a_piece_bytes = round_up((size_t)g.batch * (size_t)g.M * (size_t)pl->Kp * pl->elem, 1024);
+    pl->b_piece_bytes = round_up((size_t)g.batch * (size_t)g.N * (size_t)pl->Kp * pl->elem, 1024);
+    pl->mblocks = pl->nblocks = pl->kblocks = 0;
+    pl->sa_bytes = pl->sb_bytes = 0;
+    if (pl->mode == 3) {
+        pl->mblocks = (g.M + kQBlock - 1) / kQBlock;
+        pl->nblocks = (g.N + kQBlock - 1) / kQBlock;
+        pl->kblocks = (int64_t)((K + kQBlock - 1) / kQBlock);
+        pl->sa_bytes = round_up((size_t)g.batch * pl->mblocks * pl->kblocks * 4, 1024);
+        pl->sb_bytes = round_up((size_t)g.batch * pl->nblocks * pl->kblocks * 4, 1024);
+    }
+    pl->total = pl->np * (pl->a_piece_bytes + pl->b_piece_bytes) + pl->sa_bytes + pl->sb_bytes;
     return true;
+}
+
+static int launch_quant(bool transposed, const float *src, int64_t rows, int64_t K, int64_t Kp, int64_t ld,
+                        int64_t src_stride, int64_t batch, uint8_t *codes, float *scales, cudaStream_t stream) {
+    QuantArgs a;
+    a.src = src;
+    a.rows = rows;
+    a.K = K;
+    a.Kp = Kp;
+    a.ld = ld;
+    a.src_stride = src_stride;
+    a.transposed = transposed ? 1 : 0;
+    a.vec = (ld % 4 == 0) && aligned16(src) && (batch == 1 || src_stride % 4 == 0);
+    a.codes = codes;
+    a.scales = scales;
+    a.rblocks = (rows + kQBlock - 1) / kQBlock;
+    a.kblocks = (K + kQBlock - 1) / kQBlock;
+    if (a.rblocks > 65535) return set_error(GATLAS_ERR_INVALID, "matmul: too many rows for the FP8 pass");
+    dim3 gr((unsigned)a.kblocks, (unsigned)a.rblocks, (unsigned)batch);
+    quant_fp8_kernel<<<gr, 256, 0, stream>>>(a);
+    return check_launch("quant_fp8_kernel");
 }
 
 static int launch_split(int np, bool transposed, const float *src, int64_t rows, int64_t K, int64_t Kp,
@@ -440,22 +643,47 @@ static int launch_split(int np, bool transposed, const float *src, int64_t rows,
     return check_launch("split kernel");
 }
 
+// Operand pointers inside a prepared workspace: [A pieces][B pieces], then
+// for FP8 [A scales][B scales].
+struct WsPtrs {
+    void *a[3], *b[3];
+    float *sa, *sb;
+};
+
+static WsPtrs ws_ptrs(const Plan &pl, void *ws) {
+    uint8_t *base = static_cast<uint8_t *>(ws);
+    WsPtrs w;
+    for (int i = 0; i < 3; ++i) {
+        w.a[i] = w.b[i] = nullptr;
+        if (i < pl.np) {
+            w.a[i] = base + i * pl.a_piece_bytes;
+            w.b[i] = base + pl.np * pl.a_piece_bytes + i * pl.b_piece_bytes;
+        }
+    }
+    uint8_t *sc = base + pl.np * (pl.a_piece_bytes + pl.b_piece_bytes);
+    w.sa = pl.mode == 3 ? reinterpret_cast<float *>(sc) : nullptr;
+    w.sb = pl.mode == 3 ? reinterpret_cast<float *>(sc + pl.sa_bytes) : nullptr;
+    return w;
+}
+
 template <int MODE>
-static int launch_tc(const Geometry &g, const Plan &pl, __nv_bfloat16 *const ap[3], __nv_bfloat16 *const bp[3],
-                     float *C, double alpha, double beta, int gemm, int seg_kblocks, cudaStream_t stream) {
+static int launch_tc(const Geometry &g, const Plan &pl, const WsPtrs &w, float *C, double alpha, double beta,
+                     int gemm, int seg_kblocks, cudaStream_t stream) {
+    using L = Layout<MODE>;
     CUtensorMap ta[3], tb[3];
+    const uint64_t row_bytes = (uint64_t)pl.Kp * pl.elem;
     const uint64_t adims[3] = {(uint64_t)pl.Kp, (uint64_t)g.M, (uint64_t)g.batch};
-    const uint64_t astr[2] = {(uint64_t)pl.Kp * 2, (uint64_t)pl.Kp * 2 * (uint64_t)g.M};
+    const uint64_t astr[2] = {row_bytes, row_bytes * (uint64_t)g.M};
     const uint64_t bdims[3] = {(uint64_t)pl.Kp, (uint64_t)g.N, (uint64_t)g.batch};
-    const uint64_t bstr[2] = {(uint64_t)pl.Kp * 2, (uint64_t)pl.Kp * 2 * (uint64_t)g.N};
-    const uint32_t abox[3] = {BK, BM, 1}, bbox[3] = {BK, BN, 1};
+    const uint64_t bstr[2] = {row_bytes, row_bytes * (uint64_t)g.N};
+    const uint32_t abox[3] = {(uint32_t)L::BK, BM, 1}, bbox[3] = {(uint32_t)L::BK, BN, 1};
+    const CUtensorMapDataType dt = MODE == 3 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    const CUtensorMapSwizzle swz = L::ROW_BYTES == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
     for (int i = 0; i < 3; ++i) {
         const int src = i < pl.np ? i : 0;  // unused slots alias piece 0
-        int rc = make_tensor_map(&ta[i], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, ap[src], adims, astr, abox,
-                                 CU_TENSOR_MAP_SWIZZLE_64B);
+        int rc = make_tensor_map(&ta[i], dt, 3, w.a[src], adims, astr, abox, swz);
         if (rc) return rc;
-        rc = make_tensor_map(&tb[i], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, bp[src], bdims, bstr, bbox,
-                             CU_TENSOR_MAP_SWIZZLE_64B);
+        rc = make_tensor_map(&tb[i], dt, 3, w.b[src], bdims, bstr, bbox, swz);
         if (rc) return rc;
     }
     Params p;
@@ -464,13 +692,19 @@ static int launch_tc(const Geometry &g, const Plan &pl, __nv_bfloat16 *const ap[
     p.N = g.N;
     p.ldc = g.ldc;
     p.stride_c = g.stride_c;
-    p.kblocks = (int)((pl.Kp + BK - 1) / BK);
-    p.seg_kblocks = seg_kblocks > 0 ? seg_kblocks : kDefaultSegKblocks;
+    p.kblocks = (int)((pl.Kp + L::BK - 1) / L::BK);
+    p.seg_kblocks = Mode<MODE>::SCALED ? 1 : (seg_kblocks > 0 ? seg_kblocks : kDefaultSegKblocks);
     p.alpha = (float)alpha;
     p.beta = (float)beta;
     p.gemm = gemm;
     p.fault = device_fault_word();
-    const int smem = (int)Layout<MODE>::SMEM_BYTES;
+    p.scale_a = w.sa;
+    p.scale_b = w.sb;
+    p.scale_a_stride = pl.mblocks * pl.kblocks;
+    p.scale_b_stride = pl.nblocks * pl.kblocks;
+    p.nblocks_n = (int)pl.nblocks;
+    if (MODE == 3 && p.kblocks != pl.kblocks) return set_error(GATLAS_ERR_INVALID, "matmul: FP8 slice count");
+    const int smem = (int)L::SMEM_BYTES;
     cudaError_t e = cudaFuncSetAttribute(tc_gemm_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "tc gemm smem attribute: %s", cudaGetErrorString(e));
     const int64_t gx = (g.N + BN - 1) / BN, gy = (g.M + BM - 1) / BM;
@@ -478,18 +712,6 @@ static int launch_tc(const Geometry &g, const Plan &pl, __nv_bfloat16 *const ap[
     dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)g.batch);
     tc_gemm_kernel<MODE><<<grid, kThreads2, smem, stream>>>(ta[0], ta[1], ta[2], tb[0], tb[1], tb[2], p);
     return check_launch("tc_gemm_kernel");
-}
-
-// Piece pointers inside a prepared workspace.
-static void piece_ptrs(const Plan &pl, void *ws, __nv_bfloat16 *ap[3], __nv_bfloat16 *bp[3]) {
-    uint8_t *base = static_cast<uint8_t *>(ws);
-    for (int i = 0; i < 3; ++i) {
-        ap[i] = bp[i] = nullptr;
-        if (i < pl.np) {
-            ap[i] = reinterpret_cast<__nv_bfloat16 *>(base + i * pl.a_piece_bytes);
-            bp[i] = reinterpret_cast<__nv_bfloat16 *>(base + pl.np * pl.a_piece_bytes + i * pl.b_piece_bytes);
-        }
-    }
 }
 
 static int check_ws(const Plan &pl, const void *ws, size_t ws_bytes) {
@@ -505,9 +727,20 @@ int tc_prepare(const gatlas_matmul_desc *d, const Geometry &g, const float *A, c
     if (!make_plan(d, g, &pl)) return set_error(GATLAS_ERR_UNSUPPORTED, "matmul: tensor-core engine %d not built", d->engine);
     int rc = check_ws(pl, ws, ws_bytes);
     if (rc) return rc;
-    __nv_bfloat16 *ap[3], *bp[3];
-    piece_ptrs(pl, ws, ap, bp);
+    const WsPtrs w = ws_ptrs(pl, ws);
     // A is K-major already when not transposed; B is K-major when transposed.
+    if (pl.mode == 3) {
+        rc = launch_quant(g.ta, A, g.M, g.K, pl.Kp, g.lda, g.stride_a, g.batch, static_cast<uint8_t *>(w.a[0]), w.sa,
+                          stream);
+        if (rc) return rc;
+        return launch_quant(!g.tb, B, g.N, g.K, pl.Kp, g.ldb, g.stride_b, g.batch, static_cast<uint8_t *>(w.b[0]),
+                            w.sb, stream);
+    }
+    __nv_bfloat16 *ap[3], *bp[3];
+    for (int i = 0; i < 3; ++i) {
+        ap[i] = static_cast<__nv_bfloat16 *>(w.a[i]);
+        bp[i] = static_cast<__nv_bfloat16 *>(w.b[i]);
+    }
     rc = launch_split(pl.np, g.ta, A, g.M, g.K, pl.Kp, g.lda, g.stride_a, g.batch, ap, stream);
     if (rc) return rc;
     return launch_split(pl.np, !g.tb, B, g.N, g.K, pl.Kp, g.ldb, g.stride_b, g.batch, bp, stream);
@@ -520,12 +753,12 @@ int tc_run(const gatlas_matmul_desc *d, const Geometry &g, const void *ws, size_
     int rc = check_ws(pl, ws, ws_bytes);
     if (rc) return rc;
     if (g.K == 0) return set_error(GATLAS_ERR_INVALID, "matmul: K == 0 has no prepared operands");
-    __nv_bfloat16 *ap[3], *bp[3];
-    piece_ptrs(pl, const_cast<void *>(ws), ap, bp);
+    const WsPtrs w = ws_ptrs(pl, const_cast<void *>(ws));
     switch (pl.mode) {
-        case 0: return launch_tc<0>(g, pl, ap, bp, C, d->alpha, d->beta, d->gemm, (int)d->extra, stream);
-        case 1: return launch_tc<1>(g, pl, ap, bp, C, d->alpha, d->beta, d->gemm, (int)d->extra, stream);
-        default: return launch_tc<2>(g, pl, ap, bp, C, d->alpha, d->beta, d->gemm, (int)d->extra, stream);
+        case 0: return launch_tc<0>(g, pl, w, C, d->alpha, d->beta, d->gemm, (int)d->extra, stream);
+        case 1: return launch_tc<1>(g, pl, w, C, d->alpha, d->beta, d->gemm, (int)d->extra, stream);
+        case 2: return launch_tc<2>(g, pl, w, C, d->alpha, d->beta, d->gemm, (int)d->extra, stream);
+        default: return launch_tc<3>(g, pl, w, C, d->alpha, d->beta, d->gemm, (int)d->extra, stream);
     }
 }
 
@@ -539,7 +772,7 @@ size_t tc_workspace_bytes(const gatlas_matmul_desc *d, const Geometry &g) {
 
 int tc_supported(const gatlas_matmul_desc *d) {
     return d->engine == GATLAS_ENGINE_TC_BF16 || d->engine == GATLAS_ENGINE_TC_SPLIT3 ||
-           d->engine == GATLAS_ENGINE_TC_SPLIT6;
+           d->engine == GATLAS_ENGINE_TC_SPLIT6 || d->engine == GATLAS_ENGINE_TC_FP8;
 }
 
 int matmul_tc(const gatlas_matmul_desc *d, const Geometry &g, const float *A, const float *B, float *C, void *ws,

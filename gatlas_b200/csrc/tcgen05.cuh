@@ -4,9 +4,10 @@
 //   leading-dimension byte offset >> 4 [16,30), stride-dimension byte offset
 //   >> 4 [32,46), descriptor version 1 [46,48), base offset [49,52), layout
 //   (swizzle) type [61,64) with 0 = none, 2 = 128B, 4 = 64B, 6 = 32B;
-//   instruction descriptor for kind::f16 (32 bit): D format [4,6) (1 = F32),
-//   A format [7,10) and B format [10,13) (0 = F16, 1 = BF16), A/B major
-//   [15], [16] (0 = K-major), N >> 3 [17,23), M >> 4 [24,29).
+//   instruction descriptor for kind::f16 and kind::f8f6f4 (32 bit): D format
+//   [4,6) (1 = F32), A format [7,10) and B format [10,13) (kind::f16: 0 = F16,
+//   1 = BF16; kind::f8f6f4: 0 = E4M3, 1 = E5M2), A/B major [15], [16]
+//   (0 = K-major), N >> 3 [17,23), M >> 4 [24,29).
 #pragma once
 
 #include <stdint.h>
@@ -60,6 +61,15 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
            | ((uint32_t)(M >> 4) << 24);// M
 }
 
+// kind::f8f6f4 with A = B = E4M3 (format code 0) and an F32 accumulator.
+__host__ __device__ constexpr uint32_t idesc_e4m3_f32(int M, int N) {
+    return (1u << 4)                    // D = F32
+           | (0u << 7)                  // A = E4M3
+           | (0u << 10)                 // B = E4M3
+           | ((uint32_t)(N >> 3) << 17) // N
+           | ((uint32_t)(M >> 4) << 24);// M
+}
+
 __device__ __forceinline__ void tmem_alloc(uint32_t *smem_dst, uint32_t ncols) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(smem_dst)),
                  "r"(ncols)
@@ -89,6 +99,17 @@ __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint6
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// D[tmem] (+)= A * B^T with 8-bit floating-point operands (K = 32 per instruction).
+__device__ __forceinline__ void mma_f8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                       uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
         "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
         : "memory");
 }

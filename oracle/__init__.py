@@ -66,6 +66,11 @@ def lib() -> ctypes.CDLL:
         L.oracle_check_pattern_f32.argtypes = [vp, c_sz, ctypes.c_float]
         L.oracle_check_pattern_f64.argtypes = [vp, c_sz, ctypes.c_double]
         L.oracle_max_threads.restype = c_int
+        L.oracle_e4m3_encode_n.argtypes = [vp, vp, c_sz]
+        L.oracle_e4m3_decode_n.argtypes = [vp, vp, c_sz]
+        L.oracle_quant_fp8.argtypes = [c_sz, c_sz, c_sz, c_sz, c_int, c_sz, c_sz, vp, vp, vp]
+        L.oracle_matmul_fp8_dequant.argtypes = [c_sz, c_int, c_sz, c_sz, c_sz, c_sz, vp, vp, vp, vp,
+                                                ctypes.c_double, ctypes.c_double, vp, vp]
         _lib = L
     return _lib
 
@@ -206,3 +211,58 @@ def normwise_error(C, Cref, A=None, B=None) -> float:
     else:
         den = np.linalg.norm(Cref.ravel())
     return float(num / den) if den else float(num)
+
+
+# ---- FP8 E4M3 block quantisation --------------------------------------------
+
+FP8_BLOCK = 128
+
+
+def e4m3_encode(x) -> np.ndarray:
+    x = _c(x, np.float32).ravel()
+    out = np.empty(x.size, dtype=np.uint8)
+    lib().oracle_e4m3_encode_n(_p(x), _p(out), x.size)
+    return out
+
+
+def e4m3_decode(c) -> np.ndarray:
+    c = _c(c, np.uint8).ravel()
+    out = np.empty(c.size, dtype=np.float32)
+    lib().oracle_e4m3_decode_n(_p(c), _p(out), c.size)
+    return out
+
+
+def fp8_kp(K: int) -> int:
+    """Row pitch (in codes) of the K-major FP8 operand: K rounded up to 16."""
+    return (max(K, 1) + 15) // 16 * 16
+
+
+def quant_fp8(src, rows: int, K: int, transposed: int, ld: int | None = None, batch: int = 1,
+              src_stride: int | None = None):
+    """Block quantisation of one operand viewed as rows x K (element (r,k) at
+    src[r*ld + k], or src[k*ld + r] when transposed).  Returns (codes
+    [batch, rows, Kp] uint8, scales [batch, rblocks, kblocks] float32)."""
+    src = _c(src, np.float32).ravel()
+    ld = ld if ld is not None else (rows if transposed else K)
+    src_stride = src_stride if src_stride is not None else rows * K
+    Kp = fp8_kp(K)
+    rb, kb = -(-rows // FP8_BLOCK), -(-max(K, 1) // FP8_BLOCK)
+    codes = np.zeros((batch, rows, Kp), dtype=np.uint8)
+    scales = np.zeros((batch, rb, kb), dtype=np.float32)
+    assert lib().oracle_quant_fp8(batch, rows, K, Kp, transposed, ld, src_stride, _p(src), _p(codes),
+                                  _p(scales)) == 0
+    return codes, scales
+
+
+def matmul_fp8_dequant(qa, sa, qb, sb, M: int, N: int, K: int, batch: int = 1, gemm: int = 0,
+                       alpha: float = 1.0, beta: float = 0.0, Cin=None) -> np.ndarray:
+    """FP64 product of the dequantised operands (codes K-major: A as M x Kp, B as N x Kp)."""
+    qa, qb = _c(qa, np.uint8), _c(qb, np.uint8)
+    sa, sb = _c(sa, np.float32), _c(sb, np.float32)
+    Ci = None if Cin is None else _c(Cin, np.float32).ravel()
+    if gemm and Ci is None:
+        Ci = np.zeros(batch * M * N, dtype=np.float32)
+    out = np.empty(batch * M * N, dtype=np.float64)
+    lib().oracle_matmul_fp8_dequant(batch, gemm, M, N, K, fp8_kp(K), _p(qa), _p(sa), _p(qb), _p(sb),
+                                    alpha, beta, _p(Ci), _p(out))
+    return out

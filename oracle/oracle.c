@@ -421,3 +421,109 @@ int oracle_check_pattern_f64(const double *a, size_t n, double value) {
         if (a[i] != value) return 0;
     return 1;
 }
+
+/* ----------------------------------------------------------------------- */
+/* FP8 E4M3 block quantisation and the dequantised product                  */
+/* ----------------------------------------------------------------------- */
+
+uint8_t oracle_e4m3_encode(float x) {
+    if (isnan(x)) return 0x7F;
+    const uint8_t sign = signbit(x) ? 0x80 : 0x00;
+    const double a = fabs((double)x);
+    if (a >= 448.0) return sign | 0x7E; /* saturate */
+    int code;
+    if (a < 0x1p-6) {
+        /* subnormal quantum 2^-9; a result of 8 is the smallest normal 0x08 */
+        code = (int)nearbyint(a * 0x1p9);
+    } else {
+        int e;
+        frexp(a, &e);            /* a = f * 2^e, f in [0.5, 1) */
+        const int E = e - 1;     /* floor(log2 a), in [-6, 8] */
+        const int mm = (int)nearbyint(ldexp(a, 3 - E)); /* 8..16; 16 carries into the exponent */
+        code = ((E + 7) << 3) + mm - 8;
+    }
+    return sign | (uint8_t)code;
+}
+
+float oracle_e4m3_decode(uint8_t c) {
+    const int e = (c >> 3) & 15, m = c & 7;
+    if (e == 15 && m == 7) return NAN;
+    const double v = e == 0 ? ldexp((double)m, -9) : ldexp((double)(8 + m), e - 10);
+    return (float)((c & 0x80) ? -v : v);
+}
+
+void oracle_e4m3_encode_n(const float *x, uint8_t *out, size_t n) {
+    for (size_t i = 0; i < n; i++) out[i] = oracle_e4m3_encode(x[i]);
+}
+
+void oracle_e4m3_decode_n(const uint8_t *c, float *out, size_t n) {
+    for (size_t i = 0; i < n; i++) out[i] = oracle_e4m3_decode(c[i]);
+}
+
+#define QB 128
+
+int oracle_quant_fp8(size_t batch, size_t rows, size_t K, size_t Kp, int transposed, size_t ld,
+                     size_t src_stride, const float *src, uint8_t *codes, float *scales) {
+    if (Kp < K) return -1;
+    const size_t rblocks = (rows + QB - 1) / QB, kblocks = (K + QB - 1) / QB;
+    for (size_t z = 0; z < batch; z++) {
+        const float *s0 = src + z * src_stride;
+        uint8_t *c0 = codes + z * rows * Kp;
+        for (size_t rb = 0; rb < rblocks; rb++)
+            for (size_t kb = 0; kb < kblocks; kb++) {
+                const size_t r_end = rb * QB + QB < rows ? rb * QB + QB : rows;
+                const size_t k_end = kb * QB + QB < K ? kb * QB + QB : K;
+                float amax = 0.0f;
+                for (size_t r = rb * QB; r < r_end; r++)
+                    for (size_t k = kb * QB; k < k_end; k++) {
+                        const float x = transposed ? s0[k * ld + r] : s0[r * ld + k];
+                        const float ax = fabsf(x);
+                        if (ax > amax) amax = ax;
+                    }
+                /* smallest power of two with amax / s <= 448 */
+                float s = 0.0f;
+                if (amax > 0.0f) {
+                    int e;
+                    const float f = frexpf(amax, &e);
+                    s = ldexpf(1.0f, e - 9 + (f > 0.875f ? 1 : 0));
+                }
+                scales[(z * rblocks + rb) * kblocks + kb] = s;
+                /* codes of this block, including the zero padding up to Kp
+                 * that falls inside the last block */
+                const size_t kc_end = kb + 1 == kblocks ? Kp : kb * QB + QB;
+                for (size_t r = rb * QB; r < r_end; r++)
+                    for (size_t k = kb * QB; k < kc_end; k++) {
+                        const float x = k < K ? (transposed ? s0[k * ld + r] : s0[r * ld + k]) : 0.0f;
+                        c0[r * Kp + k] = s == 0.0f ? 0 : oracle_e4m3_encode(x / s);
+                    }
+            }
+    }
+    return 0;
+}
+
+int oracle_matmul_fp8_dequant(size_t batch, int gemm, size_t M, size_t N, size_t K, size_t Kp,
+                              const uint8_t *qa, const float *sa, const uint8_t *qb, const float *sb,
+                              double alpha, double beta, const float *Cin, double *out) {
+    const size_t kblocks = (K + QB - 1) / QB, mblocks = (M + QB - 1) / QB, nblocks = (N + QB - 1) / QB;
+    float lut[256];
+    for (int c = 0; c < 256; c++) lut[c] = oracle_e4m3_decode((uint8_t)c);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (size_t z = 0; z < batch; z++)
+        for (size_t m = 0; m < M; m++) {
+            const uint8_t *arow = qa + (z * M + m) * Kp;
+            for (size_t n = 0; n < N; n++) {
+                const uint8_t *brow = qb + (z * N + n) * Kp;
+                double acc = 0.0;
+                for (size_t kb = 0; kb < kblocks; kb++) {
+                    double part = 0.0;
+                    const size_t k_end = kb * QB + QB < K ? kb * QB + QB : K;
+                    for (size_t k = kb * QB; k < k_end; k++) part += (double)lut[arow[k]] * (double)lut[brow[k]];
+                    acc += part * (double)sa[(z * mblocks + m / QB) * kblocks + kb] *
+                           (double)sb[(z * nblocks + n / QB) * kblocks + kb];
+                }
+                const size_t o = (z * M + m) * N + n;
+                out[o] = gemm ? alpha * acc + beta * (double)Cin[o] : acc;
+            }
+        }
+    return 0;
+}

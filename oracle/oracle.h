@@ -80,6 +80,26 @@ int oracle_saxpy_f64(int mode, size_t n, double alpha, const double *x, const do
                      double *z, int threads);
 
 /* ---- checks (OCLAppUtil.hpp:47-61, 212-264) ---------------------------- */
+/* FP8 E4M3 operands of the tensor-core FP8 engine (no reference
+ * counterpart: the reference has no 8-bit path).  Encoding: 1 sign, 4
+ * exponent bits (bias 7), 3 mantissa bits, no infinities, 0x7F/0xFF NaN,
+ * largest finite 448; rounding to nearest even with saturation to +-448.
+ * Block quantisation: one FP32 scale per 128 x 128 block of the K-major
+ * operand (rows x K), s = the smallest power of two with amax / s <= 448,
+ * code = e4m3(x / s), s = 0 and all codes 0 for an all-zero block; codes
+ * laid out [batch][rows][Kp], zero for k >= K. */
+uint8_t oracle_e4m3_encode(float x);
+float   oracle_e4m3_decode(uint8_t c);
+void    oracle_e4m3_encode_n(const float *x, uint8_t *out, size_t n);
+void    oracle_e4m3_decode_n(const uint8_t *c, float *out, size_t n);
+int oracle_quant_fp8(size_t batch, size_t rows, size_t K, size_t Kp, int transposed, size_t ld,
+                     size_t src_stride, const float *src, uint8_t *codes, float *scales);
+/* C = sum over K blocks of sa*sb * (sum of decoded code products), in FP64,
+ * with alpha/beta applied when gemm != 0 (Cin read then). */
+int oracle_matmul_fp8_dequant(size_t batch, int gemm, size_t M, size_t N, size_t K, size_t Kp,
+                              const uint8_t *qa, const float *sa, const uint8_t *qb, const float *sb,
+                              double alpha, double beta, const float *Cin, double *out);
+
 long double oracle_absdiff_f32(const float *a, const float *b, size_t n);
 long double oracle_absdiff_f64(const double *a, const double *b, size_t n);
 int oracle_check_pattern_f32(const float *a, size_t n, float value);

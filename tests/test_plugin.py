@@ -104,7 +104,7 @@ def test_reference_printed_points_through_plugin():
 
 def test_tensor_core_types():
     for t, name in (("tcbf16", "matmultcbf16float4"), ("split3", "matmultcsplit3float4"),
-                    ("split6", "matmultcsplit6float4")):
+                    ("split6", "matmultcsplit6float4"), ("fp8", "matmultcfp8float4")):
         assert Kernel("matmul", t).kernel_name() == name
     with pytest.raises(Exception):
         Kernel("matvec", "split3")

@@ -25,6 +25,8 @@ def run(args):
     ("split3", [1, 0, 512, 512, 512, 0, 0, 16, 16, 8, 4, 0]),
     ("split6", [1, 1, 256, 256, 256, 1, 0, 16, 16, 8, 4, 0]),
     ("tcbf16", [1, 0, 256, 512, 128, 0, 1, 16, 16, 8, 4, 0]),
+    ("fp8", [1, 0, 512, 512, 512, 0, 0, 16, 16, 8, 4, 0]),
+    ("fp8", [2, 1, 256, 384, 640, 1, 0, 16, 16, 8, 4, 0]),
     ("floatimg", [1, 0, 512, 512, 512, 0, 0, 16, 16, 8, 4, 0]),
     ("floatimg", [1, 1, 256, 256, 256, 1, 1, 16, 16, 4, 4, 3]),
     ("doubleimg", [1, 0, 256, 256, 256, 1, 0, 16, 16, 4, 4, 0]),
