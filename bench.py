@@ -178,6 +178,92 @@ def _timed(fn, steps, warmup, world, stream):
     return start.elapsed_time(stop) / steps  # ms per step
 
 
+GROUPED_INSTANCES = 1024
+
+
+def grouped_workload(dev, count=GROUPED_INSTANCES, seed=4, lo=16, hi=4096):
+    """The batched uneven workload: m, n, k log-uniform in [lo, hi] rounded to
+    multiples of 16, random layouts, alpha uniform [0.5, 2], beta in {0, 1}.
+    Operands live in three device buffers (instance offsets 64-byte aligned),
+    filled with seeded uniform[-1,1) values."""
+    import numpy as np
+    import torch
+
+    import gatlas_b200 as g
+    rng = np.random.default_rng(seed)
+
+    def lu(n):
+        v = np.exp(rng.uniform(np.log(lo), np.log(hi), n))
+        return np.clip(np.round(v / 16) * 16, lo, hi).astype(np.int64)
+    m, n, k = lu(count), lu(count), lu(count)
+    ta, tb = rng.integers(0, 2, count), rng.integers(0, 2, count)
+    alpha, beta = rng.uniform(0.5, 2.0, count), rng.integers(0, 2, count).astype(float)
+    r16 = lambda x: (int(x) + 15) // 16 * 16
+    sa, sb, sc = (sum(r16(a * b) for a, b in zip(x, y)) for x, y in ((m, k), (k, n), (m, n)))
+    A = torch.empty(sa, device=dev)
+    B = torch.empty(sb, device=dev)
+    C = torch.empty(sc, device=dev)
+    g.fill(A, "uniform", seed=seed + 1)
+    g.fill(B, "uniform", seed=seed + 2)
+    g.fill(C, "uniform", seed=seed + 3)
+    inst, oa, ob, oc = [], 0, 0, 0
+    for i in range(count):
+        mi, ni, ki = int(m[i]), int(n[i]), int(k[i])
+        inst.append(dict(A=A[oa:oa + mi * ki], B=B[ob:ob + ki * ni], C=C[oc:oc + mi * ni], m=mi, n=ni, k=ki,
+                         trans_a=int(ta[i]), trans_b=int(tb[i]), gemm=1, alpha=float(alpha[i]),
+                         beta=float(beta[i])))
+        oa, ob, oc = oa + r16(mi * ki), ob + r16(ki * ni), oc + r16(mi * ni)
+    return inst, (A, B, C)
+
+
+def grouped_leg(args, world, stream):
+    """Batched uneven GEMM: one persistent grouped launch per dtype in a CUDA
+    graph vs one engine call per instance."""
+    import tempfile
+
+    import numpy as np
+    import torch
+
+    import gatlas_b200 as g
+    dev = torch.cuda.current_device()
+    out = {"instances": GROUPED_INSTANCES, "shapes": "m, n, k log-uniform [16, 4096], multiples of 16",
+           "layouts": "trans_a, trans_b random", "alpha": "uniform [0.5, 2]", "beta": "{0, 1}"}
+    inst, bufs = grouped_workload(dev)
+    flops = sum(2.0 * q["m"] * q["n"] * q["k"] for q in inst)
+    out["gflop"] = flops / 1e9
+    for eng in ("tc_split3", "tc_bf16"):
+        t0 = time.time()
+        with tempfile.TemporaryDirectory() as d:
+            table = g.grouped_autotune(eng, journal=os.path.join(d, "grouped.journal"), trials=2, seed=1)
+        row = {"tile_table": table, "autotune_s": time.time() - t0}
+        plan = g.Grouped(inst, engine=eng)
+        row.update(plan.info())
+        C0 = bufs[2].clone()
+        full = _timed(lambda: plan.launch_graph(with_prepare=True), max(3, min(args.steps, 10)), 2, world, stream)
+        run = _timed(lambda: plan.launch_graph(with_prepare=False), max(3, min(args.steps, 10)), 2, world, stream)
+        each = _timed(lambda: plan.run_each(), 2, 1, world, stream)
+        # the per-instance path gives the same results (same pieces, same MMA order)
+        sample = (0, 511, GROUPED_INSTANCES - 1)
+        bufs[2].copy_(C0)
+        plan.launch_graph(with_prepare=True)
+        torch.cuda.synchronize()
+        got = [inst[i]["C"].clone() for i in sample]
+        bufs[2].copy_(C0)
+        plan.run_each()
+        torch.cuda.synchronize()
+        same = all(torch.equal(inst[i]["C"], x) for i, x in zip(sample, got))
+        del C0
+        row.update({"graph_prepare_run_ms": full, "graph_run_ms": run, "per_instance_ms": each,
+                    "tflops_graph_prepare_run": flops / (full * 1e-3) / 1e12,
+                    "tflops_graph_run": flops / (run * 1e-3) / 1e12,
+                    "tflops_per_instance": flops / (each * 1e-3) / 1e12,
+                    "speedup_vs_per_instance": each / full, "bit_identical_sample": bool(same)})
+        plan.close()
+        out[eng] = row
+    del inst, bufs
+    return out
+
+
 def _gemm_step_fn(g, A, B, C, M, N, K, engine, ws):
     def step():
         g.matmul(A, B, M, N, K, C=C, engine=engine, workspace=ws)
@@ -318,6 +404,9 @@ def run_ours(args, rank, world, local):
     secondary["hbm_peak_gbs"] = peaks["hbm_gbs"]
     del xs, ys
 
+    # ---- batched uneven GEMM (grouped persistent kernel) ------------------------
+    grouped = grouped_leg(args, world, stream) if not args.quick else None
+
     faults = g.device_faults()
     cpu = cpu_baseline(args.cpu_seconds) if (rank == 0 and world == 1 and not args.no_cpu) else None
 
@@ -334,6 +423,7 @@ def run_ours(args, rank, world, local):
                    "l2": "operands larger than L2; no flush"},
         "error_vs_fp64": {"normwise": fro / refn, "max_abs": mx},
         "e2e": e2e, "roofline": roofline, "precision_sweep": sweep, "secondary": secondary,
+        "grouped": grouped,
         "gpu_launches": launches_per_step * args.steps, "clocks": clocks,
         "device_faults": faults,
     }
@@ -417,7 +507,8 @@ def run_reference(args, rank, world):
 def run_case(spec: str) -> None:
     """Small single-kernel cases for ncu captures: NAME:SIZE, three calls each.
     tc_bf16|tc_split3|tc_split6|tc_fp8:M (M^3 GEMM, prepare once, run x3), sgemm_simt:M,
-    gemv_A:N / gemv_At:N (N^2 GEMV), saxpy_buffer:n / saxpy_image:n."""
+    gemv_A:N / gemv_At:N (N^2 GEMV), saxpy_buffer:n / saxpy_image:n,
+    grouped_tc_split3|grouped_tc_bf16:count (the batched workload)."""
     import torch
 
     import gatlas_b200 as g
@@ -457,6 +548,13 @@ def run_case(spec: str) -> None:
         g.fill(y, "uniform", seed=2)
         for _ in range(3):
             g.saxpy(0.5, x, y, out=y, engine=name.split("_")[1])
+    elif name.startswith("grouped_"):
+        # the batched workload with `size` instances, contraction launched x3
+        inst, bufs = grouped_workload(dev, count=size)
+        plan = g.Grouped(inst, engine=name.split("_", 1)[1])
+        plan.prepare()
+        for _ in range(3):
+            plan.run()
     else:
         raise SystemExit(f"unknown case {spec}")
     torch.cuda.synchronize()

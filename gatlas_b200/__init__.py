@@ -51,6 +51,16 @@ class MatvecDesc(ctypes.Structure):
                 ("alpha", ctypes.c_double), ("beta", ctypes.c_double)]
 
 
+class GroupedInstance(ctypes.Structure):
+    _fields_ = [("a", ctypes.c_void_p), ("b", ctypes.c_void_p), ("c", ctypes.c_void_p),
+                ("m", ctypes.c_int64), ("n", ctypes.c_int64), ("k", ctypes.c_int64),
+                ("lda", ctypes.c_int64), ("ldb", ctypes.c_int64), ("ldc", ctypes.c_int64),
+                ("trans_a", ctypes.c_int32), ("trans_b", ctypes.c_int32),
+                ("gemm", ctypes.c_int32), ("tile_n", ctypes.c_int32),
+                ("alpha", ctypes.c_double), ("beta", ctypes.c_double)]
+
+
+GROUPED_BUCKETS = 4
 _lib = None
 
 
@@ -88,6 +98,23 @@ def lib() -> ctypes.CDLL:
     L.gatlas_matmul_residual_f32.argtypes = [ctypes.POINTER(MatmulDesc), vp, vp, vp,
                                              ctypes.POINTER(ctypes.c_double), vp]
     L.gatlas_device_faults.argtypes = [ctypes.POINTER(ctypes.c_int), i32]
+    gi = ctypes.POINTER(GroupedInstance)
+    L.gatlas_grouped_workspace_size.argtypes = [i32, gi, ctypes.c_int32]
+    L.gatlas_grouped_workspace_size.restype = sz
+    L.gatlas_grouped_create.argtypes = [i32, gi, ctypes.c_int32, vp, sz, ctypes.POINTER(vp)]
+    for n in ("gatlas_grouped_prepare", "gatlas_grouped_run", "gatlas_grouped_run_each"):
+        getattr(L, n).argtypes = [vp, vp]
+    L.gatlas_grouped_launch_graph.argtypes = [vp, ctypes.c_int32, vp]
+    L.gatlas_grouped_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32),
+                                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]
+    L.gatlas_grouped_destroy.argtypes = [vp]
+    L.gatlas_grouped_destroy.restype = None
+    L.gatlas_grouped_bucket.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64]
+    L.gatlas_grouped_bucket.restype = ctypes.c_int32
+    L.gatlas_grouped_set_tile_table.argtypes = [i32, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]
+    L.gatlas_grouped_get_tile_table.argtypes = [i32, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]
+    L.gatlas_grouped_autotune.argtypes = [i32, ctypes.c_char_p, ctypes.c_int32, u64,
+                                          ctypes.POINTER(ctypes.c_int32)]
     _lib = L
     return L
 
@@ -268,3 +295,102 @@ def device_faults(clear=True) -> int:
     v = ctypes.c_int(0)
     check(lib().gatlas_device_faults(ctypes.byref(v), int(clear)))
     return v.value
+
+
+# ---------------------------------------------------------------------------
+# grouped GEMM: many uneven instances per persistent launch
+# ---------------------------------------------------------------------------
+
+def _grouped_instances(instances):
+    arr = (GroupedInstance * max(len(instances), 1))()
+    for i, q in enumerate(instances):
+        r = arr[i]
+        r.a = q["A"].data_ptr() if q.get("A") is not None else None
+        r.b = q["B"].data_ptr() if q.get("B") is not None else None
+        r.c = q["C"].data_ptr() if q.get("C") is not None else None
+        r.m, r.n, r.k = int(q["m"]), int(q["n"]), int(q["k"])
+        r.lda, r.ldb, r.ldc = int(q.get("lda", 0)), int(q.get("ldb", 0)), int(q.get("ldc", 0))
+        r.trans_a, r.trans_b = int(bool(q.get("trans_a", 0))), int(bool(q.get("trans_b", 0)))
+        r.gemm = int(bool(q.get("gemm", 0)))
+        r.tile_n = int(q.get("tile_n", 0))
+        r.alpha, r.beta = float(q.get("alpha", 1.0)), float(q.get("beta", 0.0))
+    return arr
+
+
+def grouped_workspace_size(instances, engine="tc_split3") -> int:
+    """Packed workspace bytes; instances as for Grouped (tensors may be omitted)."""
+    arr = _grouped_instances(instances)
+    return int(lib().gatlas_grouped_workspace_size(_engine(engine), arr, len(instances)))
+
+
+def grouped_bucket(m, n, k) -> int:
+    return int(lib().gatlas_grouped_bucket(m, n, k))
+
+
+def grouped_tile_table(engine="tc_split3", table=None):
+    """Returns the per-bucket tile widths; sets them first when `table` is given."""
+    buf = (ctypes.c_int32 * GROUPED_BUCKETS)()
+    if table is not None:
+        for i, v in enumerate(table):
+            buf[i] = int(v)
+        check(lib().gatlas_grouped_set_tile_table(_engine(engine), buf, GROUPED_BUCKETS))
+    check(lib().gatlas_grouped_get_tile_table(_engine(engine), buf, GROUPED_BUCKETS))
+    return list(buf)
+
+
+def grouped_autotune(engine="tc_split3", journal=None, trials=3, seed=1):
+    """Times tile widths 64/128/256 per size bucket, journals every candidate
+    and installs the winners; returns the table."""
+    out = (ctypes.c_int32 * GROUPED_BUCKETS)()
+    check(lib().gatlas_grouped_autotune(_engine(engine), journal.encode() if journal else None, trials, seed,
+                                        out))
+    return list(out)
+
+
+class Grouped:
+    """A grouped GEMM plan over instances given as dicts with keys A, B, C
+    (device float32 tensors), m, n, k and optionally lda, ldb, ldc, trans_a,
+    trans_b, gemm, alpha, beta, tile_n.  The tensors are bound at creation."""
+
+    def __init__(self, instances, engine="tc_split3", workspace=None):
+        self._keep = [(q.get("A"), q.get("B"), q.get("C")) for q in instances]
+        self._ws = workspace
+        self.engine = engine
+        self._h = ctypes.c_void_p()
+        arr = _grouped_instances(instances)
+        wsb = 0 if workspace is None else workspace.numel() * workspace.element_size()
+        check(lib().gatlas_grouped_create(_engine(engine), arr, len(instances), _ptr(workspace), wsb,
+                                          ctypes.byref(self._h)))
+
+    def prepare(self, stream=None):
+        check(lib().gatlas_grouped_prepare(self._h, _stream(stream)))
+        return self
+
+    def run(self, stream=None):
+        check(lib().gatlas_grouped_run(self._h, _stream(stream)))
+        return self
+
+    def launch_graph(self, with_prepare=True, stream=None):
+        check(lib().gatlas_grouped_launch_graph(self._h, int(bool(with_prepare)), _stream(stream)))
+        return self
+
+    def run_each(self, stream=None):
+        check(lib().gatlas_grouped_run_each(self._h, _stream(stream)))
+        return self
+
+    def info(self) -> dict:
+        t, c, f, it = ctypes.c_int64(), ctypes.c_int32(), ctypes.c_double(), ctypes.c_int64()
+        check(lib().gatlas_grouped_info(self._h, ctypes.byref(t), ctypes.byref(c), ctypes.byref(f),
+                                        ctypes.byref(it)))
+        return {"tiles": t.value, "ctas": c.value, "flops": f.value, "pack_items": it.value}
+
+    def close(self):
+        if self._h:
+            lib().gatlas_grouped_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

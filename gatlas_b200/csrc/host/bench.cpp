@@ -15,11 +15,15 @@ namespace host {
 // ---------------------------------------------------------------------------
 // Journal (GatlasBenchmark.cpp:41-137)
 // ---------------------------------------------------------------------------
-std::string Journal::key(const KernelInterface &k, const std::vector<size_t> &params) {
+std::string Journal::key(const std::string &name, const std::vector<size_t> &params) {
     std::stringstream ss;
-    ss << k.kernelName() << "_";
+    ss << name << "_";
     for (size_t p : params) ss << p << "_";
     return ss.str();
+}
+
+std::string Journal::key(const KernelInterface &k, const std::vector<size_t> &params) {
+    return key(k.kernelName(), params);
 }
 
 bool Journal::loadMemo() {
@@ -59,23 +63,35 @@ int Journal::purgeMemo(bool deleteTimes) {
     return count;
 }
 
-int Journal::memoRunState(const KernelInterface &k, const std::vector<size_t> &params) const {
-    auto it = state_.find(key(k, params));
+int Journal::memoRunState(const std::string &name, const std::vector<size_t> &params) const {
+    auto it = state_.find(key(name, params));
     return it == state_.end() ? MISSING : it->second;
 }
 
-int Journal::memoTime(const KernelInterface &k, const std::vector<size_t> &params, size_t trial) const {
-    auto it = time_.find(key(k, params));
+int Journal::memoTime(const std::string &name, const std::vector<size_t> &params, size_t trial) const {
+    auto it = time_.find(key(name, params));
     if (it == time_.end() || trial >= it->second.size()) return -1;
     return (int)it->second[trial];
 }
 
-bool Journal::takeMemo(const KernelInterface &k, const std::vector<size_t> &params, int value) const {
+bool Journal::takeMemo(const std::string &name, const std::vector<size_t> &params, int value) const {
     // append and close on every record, so a crash loses nothing already written
     std::ofstream out(file_.c_str(), std::ios::app);
     if (!out.is_open()) return false;
-    out << key(k, params) << "\t" << value << std::endl;
+    out << key(name, params) << "\t" << value << std::endl;
     return true;
+}
+
+int Journal::memoRunState(const KernelInterface &k, const std::vector<size_t> &params) const {
+    return memoRunState(k.kernelName(), params);
+}
+
+int Journal::memoTime(const KernelInterface &k, const std::vector<size_t> &params, size_t trial) const {
+    return memoTime(k.kernelName(), params, trial);
+}
+
+bool Journal::takeMemo(const KernelInterface &k, const std::vector<size_t> &params, int value) const {
+    return takeMemo(k.kernelName(), params, value);
 }
 
 // ---------------------------------------------------------------------------

@@ -35,6 +35,13 @@ class Journal {
 
     static std::string key(const KernelInterface &k, const std::vector<size_t> &params);
 
+    // The same records for a search whose subject is not a KernelInterface
+    // (the grouped engine's tile tuner): `name` stands for kernelName().
+    int memoRunState(const std::string &name, const std::vector<size_t> &params) const;
+    int memoTime(const std::string &name, const std::vector<size_t> &params, size_t trialNumber) const;
+    bool takeMemo(const std::string &name, const std::vector<size_t> &params, int value) const;
+    static std::string key(const std::string &name, const std::vector<size_t> &params);
+
   private:
     std::string file_;
     std::map<std::string, int> state_;                  // all keys

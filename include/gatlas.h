@@ -167,6 +167,67 @@ int gatlas_matmul_tc_run(const gatlas_matmul_desc *d, const void *workspace, siz
  * use (NVRTC, cached per device); 0 if it cannot run. */
 int gatlas_matmul_supported(int scalar, const gatlas_matmul_desc *d);
 
+/* ---- grouped GEMM --------------------------------------------------------
+ * Many instances of different shapes and layouts in one persistent
+ * tensor-core launch (engines GATLAS_ENGINE_TC_BF16 and
+ * GATLAS_ENGINE_TC_SPLIT3).  Replaces what the reference can only do with
+ * one kernel per problem: packedCalc batches equal shapes only
+ * (KernelMatmulBuffer.hpp:229-230, benchMatmul.cpp -C).
+ *
+ * Lifetime: create (validates, lays out the packed workspace, balances the
+ * output tiles over the SMs and uploads the tables; synchronous), then
+ * prepare (one launch packing every operand into BF16 piece tiles) and run
+ * (one launch contracting every instance), or launch_graph, which captures
+ * [prepare +] run once into a CUDA graph and replays it.  Operand and C
+ * pointers are bound at create and must stay valid.  run_each is the
+ * comparator: one gatlas_matmul_f32 call per instance. */
+#define GATLAS_GROUPED_BUCKETS 4
+
+typedef struct gatlas_grouped_instance {
+    const float *a, *b; /* device operands, layouts as in gatlas_matmul_desc */
+    float *c;
+    int64_t m, n, k;
+    int64_t lda, ldb, ldc; /* 0 = dense */
+    int32_t trans_a, trans_b;
+    int32_t gemm;   /* 1: C = alpha*op(A)op(B) + beta*C; 0: C = op(A)op(B) */
+    int32_t tile_n; /* output tile width 64, 128 or 256; 0 = the tuned width of the instance's bucket */
+    double alpha, beta;
+} gatlas_grouped_instance;
+
+typedef struct gatlas_grouped_plan gatlas_grouped_plan;
+
+/* Packed workspace bytes for the instances (0 on invalid input). */
+size_t gatlas_grouped_workspace_size(int engine, const gatlas_grouped_instance *inst, int32_t count);
+/* workspace == NULL: the plan allocates and owns it; otherwise 1024-byte
+ * aligned and at least gatlas_grouped_workspace_size bytes. */
+int gatlas_grouped_create(int engine, const gatlas_grouped_instance *inst, int32_t count, void *workspace,
+                          size_t workspace_bytes, gatlas_grouped_plan **plan);
+int gatlas_grouped_prepare(gatlas_grouped_plan *plan, void *stream);
+int gatlas_grouped_run(gatlas_grouped_plan *plan, void *stream);
+int gatlas_grouped_launch_graph(gatlas_grouped_plan *plan, int32_t with_prepare, void *stream);
+int gatlas_grouped_run_each(gatlas_grouped_plan *plan, void *stream);
+int gatlas_grouped_info(const gatlas_grouped_plan *plan, int64_t *tiles, int32_t *ctas, double *flops,
+                        int64_t *pack_items);
+void gatlas_grouped_destroy(gatlas_grouped_plan *plan);
+
+/* Size buckets for the tuned tile width: by n, [0,64], (64,128], (128,256],
+ * (256, inf).  The table (one width per bucket and engine) starts at
+ * {64, 128, 256, 256}; the autotuner (gatlas_grouped_autotune) rewrites it. */
+int32_t gatlas_grouped_bucket(int64_t m, int64_t n, int64_t k);
+int gatlas_grouped_set_tile_table(int engine, const int32_t *bucket_tile_n, int32_t nbuckets);
+int gatlas_grouped_get_tile_table(int engine, int32_t *bucket_tile_n, int32_t nbuckets);
+
+/* Autotunes the tile width of every bucket: a seeded synthetic group of 48
+ * instances per bucket (m, k log-uniform in [16,4096], n log-uniform in the
+ * bucket, multiples of 16, random layouts) is timed over `trials` runs at
+ * each width 64/128/256; the fastest width goes into the table (and into
+ * out_table when not NULL).  Every candidate is recorded in the journal at
+ * journal_path (NULL or "": none) with the reference's run states
+ * (GatlasBenchmark.cpp:185-288) under the key "grouped<engine>_<bucket>_
+ * <width>_48_<seed>_"; recorded times are replayed, crashed ones skipped. */
+int gatlas_grouped_autotune(int engine, const char *journal_path, int32_t trials, uint64_t seed,
+                            int32_t *out_table);
+
 /* ---- data generation and residuals ---------------------------------------
  * Seeded device-side generators (splitmix64 counter streams shared with the
  * host oracle): uniform [-1,1), sign·2^e (e in [-8,8]) or a constant. */

@@ -1,0 +1,143 @@
+"""Grouped GEMM on the GPU: one persistent tcgen05 launch over uneven
+instances.  Every instance's result is bit-identical to the single-instance
+engine's (same BF16 pieces, same MMA order, same promotion), whatever the
+tile width, the other instances in the group or the launch path (direct or
+CUDA graph), and within the engine's FP64 error budget."""
+import numpy as np
+import pytest
+
+import gatlas_b200 as g
+import oracle
+
+pytestmark = pytest.mark.gpu
+BUDGET = {"tc_bf16": 2.0 ** -7, "tc_split3": 8e-6}
+
+
+def _make(cuda, shapes, seed=1):
+    """shapes: (m, n, k, ta, tb, gemm, alpha, beta, tile_n).  Returns instances with
+    host copies of the inputs."""
+    import torch
+    inst = []
+    for i, (m, n, k, ta, tb, gemm, alpha, beta, tn) in enumerate(shapes):
+        A = oracle.uniform(m * k, seed=seed + 3 * i)
+        B = oracle.uniform(k * n, seed=seed + 3 * i + 1)
+        C0 = oracle.uniform(m * n, seed=seed + 3 * i + 2)
+        inst.append(dict(A=torch.from_numpy(A).to(cuda), B=torch.from_numpy(B).to(cuda),
+                         C=torch.from_numpy(C0.copy()).to(cuda), m=m, n=n, k=k, trans_a=ta, trans_b=tb,
+                         gemm=gemm, alpha=alpha, beta=beta, tile_n=tn, hA=A, hB=B, hC0=C0))
+    return inst
+
+
+def _reset(inst):
+    import torch
+    for q in inst:
+        q["C"].copy_(torch.from_numpy(q["hC0"]))
+
+
+def _results(inst):
+    import torch
+    torch.cuda.synchronize()
+    assert g.device_faults() == 0
+    return [q["C"].cpu().numpy().copy() for q in inst]
+
+
+SHAPES = [
+    (128, 256, 64, 0, 0, 0, 1.0, 0.0, 0), (200, 300, 100, 0, 1, 1, 0.5, 1.0, 0), (33, 17, 5, 1, 0, 0, 1.0, 0.0, 64),
+    (257, 129, 520, 1, 1, 1, 2.0, 0.0, 128), (16, 4000, 48, 0, 0, 1, 1.5, 1.0, 256), (1000, 16, 700, 1, 0, 0, 1.0, 0.0, 0),
+    (64, 64, 1, 0, 1, 0, 1.0, 0.0, 64), (300, 500, 0, 0, 0, 1, 1.0, 0.5, 0), (0, 50, 50, 0, 0, 0, 1.0, 0.0, 0),
+    (130, 70, 90, 1, 1, 1, 0.75, 1.0, 128), (512, 512, 256, 0, 0, 0, 1.0, 0.0, 256), (96, 1024, 33, 1, 0, 1, 1.0, 1.0, 0),
+]
+
+
+@pytest.mark.parametrize("engine", ["tc_bf16", "tc_split3"])
+def test_grouped_equals_single_instance_engine(cuda, engine):
+    inst = _make(cuda, SHAPES)
+    plan = g.Grouped(inst, engine=engine)
+    plan.prepare().run()
+    got = _results(inst)
+    _reset(inst)
+    plan.run_each()
+    want = _results(inst)
+    for q, x, y in zip(inst, got, want):
+        assert np.array_equal(x, y), (q["m"], q["n"], q["k"])
+        if q["m"] and q["n"]:
+            ref = oracle.matmul(q["hA"], q["hB"], q["m"], q["n"], q["k"], q["trans_a"], q["trans_b"], mode=oracle.F64,
+                                gemm=q["gemm"], Cin=q["hC0"], alpha=q["alpha"], beta=q["beta"])
+            assert oracle.normwise_error(x, ref) <= BUDGET[engine]
+    info = plan.info()
+    assert info["ctas"] <= 148 and info["tiles"] > 0
+    plan.close()
+
+
+@pytest.mark.parametrize("tile_n", [64, 128, 256])
+def test_result_independent_of_tile_width(cuda, tile_n):
+    shapes = [(200, 300, 100, 0, 1, 1, 0.5, 1.0, tile_n), (77, 45, 260, 1, 0, 0, 1.0, 0.0, tile_n)]
+    inst = _make(cuda, shapes, seed=5)
+    g.Grouped(inst, engine="tc_split3").prepare().run()
+    got = _results(inst)
+    _reset(inst)
+    for q in inst:
+        q["tile_n"] = 256
+    g.Grouped(inst, engine="tc_split3").prepare().run()
+    assert all(np.array_equal(x, y) for x, y in zip(got, _results(inst)))
+
+
+def test_same_result_alone_and_in_the_mix(cuda):
+    rng = np.random.default_rng(3)
+    shapes = [(int(rng.integers(16, 600)), int(rng.integers(16, 600)), int(rng.integers(16, 600)),
+               int(rng.integers(0, 2)), int(rng.integers(0, 2)), 1, 1.0, float(rng.integers(0, 2)), 0)
+              for _ in range(60)]
+    inst = _make(cuda, shapes, seed=9)
+    g.Grouped(inst, engine="tc_split3").prepare().run()
+    mixed = _results(inst)
+    for i in (0, 17, 59):
+        _reset(inst)
+        g.Grouped([inst[i]], engine="tc_split3").prepare().run()
+        assert np.array_equal(_results([inst[i]])[0], mixed[i])
+
+
+def test_graph_launch_matches_direct_and_replays(cuda):
+    inst = _make(cuda, SHAPES[:6], seed=11)
+    plan = g.Grouped(inst, engine="tc_split3")
+    plan.prepare().run()
+    direct = _results(inst)
+    for _ in range(3):
+        _reset(inst)
+        plan.launch_graph(with_prepare=True)
+        assert all(np.array_equal(x, y) for x, y in zip(direct, _results(inst)))
+    _reset(inst)
+    plan.launch_graph(with_prepare=False)          # packed operands are still resident
+    assert all(np.array_equal(x, y) for x, y in zip(direct, _results(inst)))
+
+
+def test_caller_workspace(cuda):
+    import torch
+    inst = _make(cuda, SHAPES[:4], seed=13)
+    need = g.grouped_workspace_size(inst, "tc_split3")
+    ws = torch.empty(need + 1024, dtype=torch.uint8, device=cuda)
+    ws = ws[(-ws.data_ptr()) % 1024:][:need]
+    g.Grouped(inst, engine="tc_split3", workspace=ws).prepare().run()
+    got = _results(inst)
+    _reset(inst)
+    g.Grouped(inst, engine="tc_split3").prepare().run()
+    assert all(np.array_equal(x, y) for x, y in zip(got, _results(inst)))
+    with pytest.raises(g.GatlasError):
+        g.Grouped(inst, engine="tc_split3", workspace=ws[:1024])
+
+
+def test_autotune_journals_and_replays(cuda, tmp_path):
+    from oracle.params import BUILD_IN_PROGRESS, BUILD_OK, RUN_IN_PROGRESS, RUN_OK
+    j = tmp_path / "grouped.journal"
+    old = g.grouped_tile_table("tc_bf16")
+    try:
+        table = g.grouped_autotune("tc_bf16", journal=str(j), trials=1, seed=3)
+        assert all(t in (64, 128, 256) for t in table)
+        lines = [ln.split("\t") for ln in j.read_text().splitlines()]
+        assert len(lines) == 4 * 3 * 5
+        assert [int(v) for _, v in lines[:4]] == [BUILD_IN_PROGRESS, BUILD_OK, RUN_IN_PROGRESS, RUN_OK]
+        assert lines[0][0] == "groupedtcbf16_0_64_48_3_"
+        # resumed: every candidate replayed from the journal, same decision
+        assert g.grouped_autotune("tc_bf16", journal=str(j), trials=1, seed=3) == table
+        assert len(j.read_text().splitlines()) == 60
+    finally:
+        g.grouped_tile_table("tc_bf16", old)
