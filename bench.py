@@ -264,6 +264,88 @@ def grouped_leg(args, world, stream):
     return out
 
 
+SERVE_RATES = (1000.0, 10000.0, 100000.0)
+SERVE_STREAM = 100000         # requests in the full stream
+SERVE_SECONDS = 4.0           # arrivals replayed per rate: min(stream, rate x seconds)
+SERVE_BUDGET = 128 << 30      # device-memory admission budget
+
+
+def serving_trace(count, rate, seed):
+    """Poisson arrivals at `rate`/s; 60% GEMM (m, n, k log-uniform [64, 8192]),
+    30% GEMV (rows, cols log-uniform [1024, 32768]), 10% SAXPY (n log-uniform
+    [2^16, 2^26]); operands uniform[-1,1) from the per-request seed."""
+    import numpy as np
+
+    import gatlas_b200 as g
+    rng = np.random.default_rng(seed)
+    req = np.zeros(count, dtype=g.request_dtype())
+    kinds = rng.choice([g.REQ_GEMM, g.REQ_GEMV, g.REQ_SAXPY], count, p=[0.6, 0.3, 0.1])
+    lu = lambda lo, hi: np.round(np.exp(rng.uniform(np.log(lo), np.log(hi), count))).astype(np.int64)
+    gm, gn, gk = lu(64, 8192), lu(64, 8192), lu(64, 8192)
+    vm, vn = lu(1024, 32768), lu(1024, 32768)
+    sn = lu(1 << 16, 1 << 26)
+    ta, tb = rng.integers(0, 2, count), rng.integers(0, 2, count)
+    is_mm, is_mv, is_ax = kinds == g.REQ_GEMM, kinds == g.REQ_GEMV, kinds == g.REQ_SAXPY
+    req["kind"] = kinds
+    req["seed"] = seed * 1000003 + np.arange(count)
+    req["arrival_ns"] = (np.cumsum(rng.exponential(1.0 / rate, count)) * 1e9).astype(np.int64)
+    req["m"] = np.where(is_mm, gm, np.where(is_mv, vm, 0))
+    req["n"] = np.where(is_mm, gn, np.where(is_mv, vn, sn))
+    req["k"] = np.where(is_mm, gk, 0)
+    req["trans_a"] = np.where(is_ax, 0, ta)
+    req["trans_b"] = np.where(is_mm, tb, 0)
+    req["alpha"] = np.where(is_ax, 0.5, 1.0)
+    return req
+
+
+def _serve_stats(req, out):
+    import numpy as np
+    ok = out["status"] == 0
+    lat = (out["done_ns"] - req["arrival_ns"])[ok] / 1e6
+    span = (out["done_ns"][ok].max() - req["arrival_ns"].min()) / 1e9
+    m, n, k = (req[f][ok].astype(np.float64) for f in ("m", "n", "k"))
+    kind = req["kind"][ok]
+    flops = float(np.where(kind == 0, 2 * m * n * k, np.where(kind == 1, 2 * m * n, 2 * n)).sum())
+    return {"completed": int(ok.sum()), "failed": int((~ok).sum()), "makespan_s": span,
+            "throughput_rps": float(ok.sum()) / span, "tflops": flops / span / 1e12,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean())}
+
+
+def serving_leg(args):
+    """Continuous batching vs a serial launch-per-request loop, per arrival rate."""
+    import gatlas_b200 as g
+    srv = g.Server(SERVE_BUDGET, engine="tc_split3")
+    out = {"budget_bytes": SERVE_BUDGET, "gemm_engine": "tc_split3",
+           "mix": "60% GEMM [64,8192]^3, 30% GEMV [1024,32768]^2, 10% SAXPY [2^16,2^26], log-uniform",
+           "sample": f"the first min({SERVE_STREAM}, rate x {SERVE_SECONDS:g} s) Poisson arrivals per rate"}
+    warm = serving_trace(200, 20000.0, seed=5)
+    for mode in ("continuous", "serial"):
+        srv.run(warm, mode)
+    for i, rate in enumerate(SERVE_RATES):
+        count = int(min(SERVE_STREAM, rate * SERVE_SECONDS))
+        req = serving_trace(count, rate, seed=7 + i)
+        row = {"requests": count}
+        for mode in ("continuous", "serial"):
+            st0 = srv.stats()
+            res = srv.run(req, mode)
+            row[mode] = _serve_stats(req, res)
+            if mode == "continuous":
+                st = srv.stats()
+                row[mode]["gemm_batches"] = st["gemm_batches"] - st0["gemm_batches"]
+                row[mode]["peak_bytes"] = st["peak_bytes"]
+                row[mode]["host_busy_s"] = (st["host_busy_ns"] - st0["host_busy_ns"]) / 1e9
+                row[mode]["host_phase_s"] = dict(zip(("harvest", "admit", "single_launch", "batch_tables",
+                                                      "batch_launch"),
+                                                     ((a - b) / 1e9 for a, b in zip(st["phase_ns"], st0["phase_ns"]))))
+        row["throughput_ratio"] = row["continuous"]["throughput_rps"] / row["serial"]["throughput_rps"]
+        row["p50_ratio"] = row["serial"]["p50_ms"] / row["continuous"]["p50_ms"]
+        row["p99_ratio"] = row["serial"]["p99_ms"] / row["continuous"]["p99_ms"]
+        out[f"rate_{int(rate)}"] = row
+    srv.close()
+    return out
+
+
 def _gemm_step_fn(g, A, B, C, M, N, K, engine, ws):
     def step():
         g.matmul(A, B, M, N, K, C=C, engine=engine, workspace=ws)
@@ -407,6 +489,9 @@ def run_ours(args, rank, world, local):
     # ---- batched uneven GEMM (grouped persistent kernel) ------------------------
     grouped = grouped_leg(args, world, stream) if not args.quick else None
 
+    # ---- serving stream (continuous batching vs serial) -------------------------
+    serving = serving_leg(args) if not args.quick else None
+
     faults = g.device_faults()
     cpu = cpu_baseline(args.cpu_seconds) if (rank == 0 and world == 1 and not args.no_cpu) else None
 
@@ -423,7 +508,7 @@ def run_ours(args, rank, world, local):
                    "l2": "operands larger than L2; no flush"},
         "error_vs_fp64": {"normwise": fro / refn, "max_abs": mx},
         "e2e": e2e, "roofline": roofline, "precision_sweep": sweep, "secondary": secondary,
-        "grouped": grouped,
+        "grouped": grouped, "serving": serving,
         "gpu_launches": launches_per_step * args.steps, "clocks": clocks,
         "device_faults": faults,
     }

@@ -61,6 +61,21 @@ class GroupedInstance(ctypes.Structure):
 
 
 GROUPED_BUCKETS = 4
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("budget_bytes", ctypes.c_size_t), ("gemm_engine", ctypes.c_int32),
+                ("max_batch", ctypes.c_int32), ("batch_target_ms", ctypes.c_double),
+                ("gemm_tflops_estimate", ctypes.c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("budget_bytes", ctypes.c_size_t), ("peak_bytes", ctypes.c_size_t),
+                ("used_bytes", ctypes.c_size_t), ("gemm_batches", ctypes.c_int64),
+                ("batched_gemms", ctypes.c_int64), ("host_busy_ns", ctypes.c_int64),
+                ("iterations", ctypes.c_int64), ("phase_ns", ctypes.c_int64 * 5)]
+
+
 _lib = None
 
 
@@ -115,6 +130,13 @@ def lib() -> ctypes.CDLL:
     L.gatlas_grouped_get_tile_table.argtypes = [i32, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]
     L.gatlas_grouped_autotune.argtypes = [i32, ctypes.c_char_p, ctypes.c_int32, u64,
                                           ctypes.POINTER(ctypes.c_int32)]
+    L.gatlas_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
+    L.gatlas_server_run.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_int32, vp]
+    L.gatlas_server_release.argtypes = [vp, vp]
+    L.gatlas_server_read.argtypes = [vp, vp, vp, ctypes.c_int64]
+    L.gatlas_server_stats.argtypes = [vp, ctypes.POINTER(ServerStats)]
+    L.gatlas_server_destroy.argtypes = [vp]
+    L.gatlas_server_destroy.restype = None
     _lib = L
     return L
 
@@ -387,6 +409,79 @@ class Grouped:
     def close(self):
         if self._h:
             lib().gatlas_grouped_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# serving: continuous batching of mixed requests under a memory budget
+# ---------------------------------------------------------------------------
+
+REQ_GEMM, REQ_GEMV, REQ_SAXPY = 0, 1, 2
+SERVE_MODES = {"continuous": 0, "serial": 1}
+
+
+def request_dtype():
+    """numpy layout of gatlas_request (72 bytes)."""
+    import numpy as np
+    return np.dtype([("kind", "<i4"), ("trans_a", "<i4"), ("trans_b", "<i4"), ("retain", "<i4"),
+                     ("m", "<i8"), ("n", "<i8"), ("k", "<i8"), ("alpha", "<f8"), ("beta", "<f8"),
+                     ("seed", "<u8"), ("arrival_ns", "<i8")], align=True)
+
+
+def result_dtype():
+    """numpy layout of gatlas_request_result (48 bytes)."""
+    import numpy as np
+    return np.dtype([("admit_ns", "<i8"), ("start_ns", "<i8"), ("done_ns", "<i8"), ("status", "<i4"),
+                     ("batch", "<i4"), ("result", "<u8"), ("result_elems", "<i8")], align=True)
+
+
+class Server:
+    """The serving loop: Server(budget_bytes).run(requests, mode) with requests
+    a numpy array of request_dtype(); returns an array of result_dtype()."""
+
+    def __init__(self, budget_bytes, engine="tc_split3", max_batch=0, batch_target_ms=0.0,
+                 gemm_tflops_estimate=0.0):
+        cfg = ServerConfig(int(budget_bytes), _engine(engine), int(max_batch), float(batch_target_ms),
+                           float(gemm_tflops_estimate))
+        self._h = ctypes.c_void_p()
+        check(lib().gatlas_server_create(ctypes.byref(cfg), ctypes.byref(self._h)))
+
+    def run(self, requests, mode="continuous"):
+        import numpy as np
+        req = np.ascontiguousarray(requests, dtype=request_dtype())
+        out = np.zeros(len(req), dtype=result_dtype())
+        check(lib().gatlas_server_run(self._h, req.ctypes.data if len(req) else None, len(req),
+                                      SERVE_MODES[mode] if isinstance(mode, str) else int(mode),
+                                      out.ctypes.data if len(req) else None))
+        return out
+
+    def read(self, result_row):
+        """Host copy of a retained result."""
+        import numpy as np
+        host = np.empty(int(result_row["result_elems"]), dtype=np.float32)
+        check(lib().gatlas_server_read(self._h, ctypes.c_void_p(int(result_row["result"])), host.ctypes.data,
+                                       host.size))
+        return host
+
+    def release(self, result_row):
+        check(lib().gatlas_server_release(self._h, ctypes.c_void_p(int(result_row["result"]))))
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        check(lib().gatlas_server_stats(self._h, ctypes.byref(st)))
+        out = {f: getattr(st, f) for f, _ in ServerStats._fields_}
+        out["phase_ns"] = list(st.phase_ns)
+        return out
+
+    def close(self):
+        if self._h:
+            lib().gatlas_server_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):

@@ -51,29 +51,6 @@ constexpr uint32_t kTmemCols = 512;       // two accumulators of up to 256 colum
 constexpr uint64_t kWaitNs = 2000000000ull;
 constexpr int kPackRows = 128;            // rows per pack item
 
-// Per-instance device record.
-struct Inst {
-    const float *src_a, *src_b;
-    uint8_t *pa[2], *pb[2];  // packed pieces
-    float *C;
-    int64_t M, N, K, lda, ldb, ldc;
-    int32_t ta, tb, gemm, bn, mt, nt, kt, pad;
-    float alpha, beta;
-};
-
-// Self-contained record of one output tile, in the order its CTA runs it:
-// the producer, the MMA issuer and the epilogue read nothing else.
-struct TileRec {
-    const uint8_t *a[2];  // piece tiles of this row block: [kt][128 rows x 64 B]
-    const uint8_t *b[2];  // piece tiles of this column block: [kt][bn rows x 64 B]
-    float *C;             // C at the tile's origin
-    int64_t ldc;
-    int32_t kt, bn, rows, cols;  // valid rows / columns of the tile
-    float alpha, beta;
-    int32_t gemm, pad;
-};
-static_assert(sizeof(TileRec) == 80, "tile record layout");
-
 // Packed byte offset of 16-byte chunk c of row `row` in K slice kb.
 __device__ __forceinline__ int64_t packed_offset(int64_t row, int kb, int c, int tr, int kt) {
     return ((row / tr) * kt + kb) * (int64_t)tr * kRowBytes + (row % tr) * kRowBytes +
@@ -471,15 +448,7 @@ int grouped_get_tile_table(int engine, int32_t *t, int32_t nb) {
     return GATLAS_OK;
 }
 
-// Resolved geometry of one instance.
-struct InstPlan {
-    int64_t M, N, K, lda, ldb, ldc;
-    int bn, mt, nt, kt;
-    size_t a_piece, b_piece;  // bytes per piece
-};
-
-static int resolve_instance(const gatlas_grouped_instance &in, int np, int slot, InstPlan *o) {
-    (void)np;
+static int resolve_instance(const gatlas_grouped_instance &in, int slot, InstPlan *o) {
     if (in.m < 0 || in.n < 0 || in.k < 0) return set_error(GATLAS_ERR_INVALID, "grouped: negative dimension");
     o->M = in.m, o->N = in.n, o->K = in.k;
     const int64_t a_inner = in.trans_a ? in.m : in.k, b_inner = in.trans_b ? in.k : in.n;
@@ -499,39 +468,185 @@ static int resolve_instance(const gatlas_grouped_instance &in, int np, int slot,
     o->nt = (int)((in.n + bn - 1) / bn);
     o->kt = (int)((in.k + grp::kBK - 1) / grp::kBK);
     if (in.m == 0 || in.n == 0) o->mt = o->nt = 0;
+    if (o->mt > 65535 || o->kt > (1 << 24)) return set_error(GATLAS_ERR_INVALID, "grouped: instance too large");
     o->a_piece = round_up((size_t)o->mt * o->kt * grp::kATileBytes, 1024);
     o->b_piece = round_up((size_t)o->nt * o->kt * bn * grp::kRowBytes, 1024);
     return GATLAS_OK;
 }
 
+static bool grouped_engine_ok(int engine) {
+    return engine == GATLAS_ENGINE_TC_BF16 || engine == GATLAS_ENGINE_TC_SPLIT3;
+}
+
+int grouped_instance_bytes(int engine, const gatlas_grouped_instance &in, size_t *bytes) {
+    if (!grouped_engine_ok(engine))
+        return set_error(GATLAS_ERR_UNSUPPORTED, "grouped: engine %d has no grouped kernel (tc_bf16, tc_split3)", engine);
+    InstPlan o{};
+    const int rc = resolve_instance(in, engine_slot(engine), &o);
+    if (rc) return rc;
+    const int np = engine == GATLAS_ENGINE_TC_SPLIT3 ? 2 : 1;
+    *bytes = np * (o.a_piece + o.b_piece);
+    return GATLAS_OK;
+}
+
+int grouped_build(int engine, const gatlas_grouped_instance *in, int32_t count, uint8_t *base,
+                  uint8_t *const *packed, GroupedTables *t) {
+    if (!grouped_engine_ok(engine))
+        return set_error(GATLAS_ERR_UNSUPPORTED, "grouped: engine %d has no grouped kernel (tc_bf16, tc_split3)", engine);
+    if (count < 0 || (count > 0 && !in)) return set_error(GATLAS_ERR_INVALID, "grouped: invalid instance list");
+    t->engine = engine;
+    t->np = engine == GATLAS_ENGINE_TC_SPLIT3 ? 2 : 1;
+    t->mode = engine == GATLAS_ENGINE_TC_SPLIT3 ? 1 : 0;
+    t->ip.assign(count, InstPlan{});
+    t->inst.assign(std::max(count, 1), grp::Inst{});
+    t->seg.assign(2 * (size_t)count + 1, 0);
+    t->flops = 0;
+    t->packed_bytes = 0;
+    struct Cand {
+        int64_t cost;
+        grp::TileRec r;
+    };
+    std::vector<Cand> cands;
+    size_t off = 0;
+    for (int i = 0; i < count; ++i) {
+        InstPlan &o = t->ip[i];
+        int rc = resolve_instance(in[i], engine_slot(engine), &o);
+        if (rc) return rc;
+        const gatlas_grouped_instance &q = in[i];
+        if (q.m > 0 && q.n > 0 && (!q.c || (q.k > 0 && (!q.a || !q.b))))
+            return set_error(GATLAS_ERR_INVALID, "grouped: instance %d has a null pointer", i);
+        uint8_t *pb = packed ? packed[i] : (base ? base + off : nullptr);
+        off += t->np * (o.a_piece + o.b_piece);
+        t->packed_bytes += t->np * (o.a_piece + o.b_piece);
+        t->flops += 2.0 * (double)q.m * (double)q.n * (double)q.k;
+        grp::Inst &I = t->inst[i];
+        std::memset(&I, 0, sizeof(I));
+        I.src_a = q.a;
+        I.src_b = q.b;
+        for (int j = 0; j < t->np && pb; ++j) {
+            I.pa[j] = pb + j * o.a_piece;
+            I.pb[j] = pb + t->np * o.a_piece + j * o.b_piece;
+        }
+        I.C = q.c;
+        I.M = o.M, I.N = o.N, I.K = o.K, I.lda = o.lda, I.ldb = o.ldb, I.ldc = o.ldc;
+        I.ta = q.trans_a != 0, I.tb = q.trans_b != 0, I.gemm = q.gemm != 0;
+        I.bn = o.bn, I.mt = o.mt, I.nt = o.nt, I.kt = o.kt;
+        I.alpha = (float)q.alpha;
+        I.beta = (float)q.beta;
+        const int64_t a_items = o.kt ? (int64_t)o.mt * o.kt : 0;  // 128 A rows per item = one A tile row block
+        const int64_t b_items = o.kt ? ((int64_t)o.nt * o.bn + grp::kPackRows - 1) / grp::kPackRows * o.kt : 0;
+        t->seg[2 * i + 1] = t->seg[2 * i] + a_items;
+        t->seg[2 * i + 2] = t->seg[2 * i + 1] + b_items;
+        // cost in bytes moved: operand tiles through shared memory plus the C
+        // tile (read too when beta != 0), plus a fixed per-tile overhead
+        const int64_t c_bytes = (int64_t)grp::BM * o.bn * 4 * ((q.gemm && q.beta != 0.0) ? 2 : 1);
+        const int64_t cost = (int64_t)o.kt * t->np * (grp::BM + o.bn) * grp::kRowBytes + c_bytes + 16384;
+        // grouped raster inside the instance: 16 tile rows per group, so the
+        // tiles that run at the same time share A and B rows through L2
+        for (int g0 = 0; g0 < o.mt; g0 += 16)
+            for (int tn = 0; tn < o.nt; ++tn)
+                for (int tm = g0; tm < std::min(o.mt, g0 + 16); ++tm) {
+                grp::TileRec r;
+                std::memset(&r, 0, sizeof(r));
+                for (int j = 0; j < t->np && pb; ++j) {
+                    r.a[j] = I.pa[j] + (size_t)tm * o.kt * grp::kATileBytes;
+                    r.b[j] = I.pb[j] + (size_t)tn * o.kt * o.bn * grp::kRowBytes;
+                }
+                r.C = q.c + (int64_t)tm * grp::BM * o.ldc + (int64_t)tn * o.bn;
+                r.ldc = o.ldc;
+                r.kt = o.kt;
+                r.bn = o.bn;
+                r.rows = (int32_t)std::min<int64_t>(grp::BM, o.M - (int64_t)tm * grp::BM);
+                r.cols = (int32_t)std::min<int64_t>(o.bn, o.N - (int64_t)tn * o.bn);
+                r.alpha = (float)q.alpha;
+                r.beta = (float)q.beta;
+                r.gemm = q.gemm != 0;
+                cands.push_back(Cand{cost, r});
+            }
+    }
+    t->nseg = 2 * count;
+    t->nitems = t->seg.back();
+    t->ntiles = (int64_t)cands.size();
+    // longest first onto the least-loaded CTA
+    std::stable_sort(cands.begin(), cands.end(), [](const Cand &a, const Cand &b) { return a.cost > b.cost; });
+    t->grid = (int)std::min<int64_t>(sm_count(), std::max<int64_t>(t->ntiles, 1));
+    std::vector<int> owner(cands.size());
+    std::vector<int32_t> count_per(t->grid, 0);
+    {
+        using E = std::pair<int64_t, int>;
+        std::priority_queue<E, std::vector<E>, std::greater<E>> heap;
+        for (int b = 0; b < t->grid; ++b) heap.push({0, b});
+        for (size_t c = 0; c < cands.size(); ++c) {
+            E e = heap.top();
+            heap.pop();
+            owner[c] = e.second;
+            ++count_per[e.second];
+            heap.push({e.first + cands[c].cost, e.second});
+        }
+    }
+    t->cta.assign(t->grid + 1, 0);
+    for (int b = 0; b < t->grid; ++b) t->cta[b + 1] = t->cta[b] + count_per[b];
+    t->tiles.assign(std::max<size_t>(cands.size(), 1), grp::TileRec{});
+    std::vector<int32_t> fill(t->cta.begin(), t->cta.end() - 1);
+    for (size_t c = 0; c < cands.size(); ++c) t->tiles[fill[owner[c]]++] = cands[c].r;
+    return GATLAS_OK;
+}
+
+int grouped_launch_pack(const GroupedTables &t, const GroupedDevice &d, cudaStream_t stream) {
+    if (t.nitems == 0) return GATLAS_OK;
+    const int64_t grid = std::min<int64_t>(t.nitems, (int64_t)sm_count() * 8);
+    const int64_t per_cta = (t.nitems + grid - 1) / grid;
+    if (t.np == 2)
+        grp::grouped_pack_kernel<2><<<(unsigned)grid, 256, 0, stream>>>(d.inst, d.seg, t.nseg, per_cta);
+    else
+        grp::grouped_pack_kernel<1><<<(unsigned)grid, 256, 0, stream>>>(d.inst, d.seg, t.nseg, per_cta);
+    return check_launch("grouped_pack_kernel");
+}
+
+template <int MODE>
+static int launch_grouped(const GroupedTables &t, const GroupedDevice &d, cudaStream_t stream) {
+    using L = tcg::Layout<MODE>;
+    grp::Params prm;
+    prm.tiles = d.tiles;
+    prm.cta_start = d.cta;
+    prm.seg_kblocks = tcg::kDefaultSegKblocks;
+    prm.fault = device_fault_word();
+    const int smem = (int)L::SMEM_BYTES;
+    static thread_local int attr_set[2] = {-1, -1};  // device whose attribute was set
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (attr_set[MODE] != dev) {
+        cudaError_t e = cudaFuncSetAttribute(grp::grouped_gemm_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "grouped smem attribute: %s", cudaGetErrorString(e));
+        attr_set[MODE] = dev;
+    }
+    grp::grouped_gemm_kernel<MODE><<<t.grid, grp::kThreads, smem, stream>>>(prm);
+    return check_launch("grouped_gemm_kernel");
+}
+
+int grouped_launch_contract(const GroupedTables &t, const GroupedDevice &d, cudaStream_t stream) {
+    if (t.ntiles == 0) return GATLAS_OK;
+    return t.mode == 1 ? launch_grouped<1>(t, d, stream) : launch_grouped<0>(t, d, stream);
+}
+
 struct GroupedPlan {
-    int engine = 0, np = 1, mode = 0;
     int count = 0;
     std::vector<gatlas_grouped_instance> in;
-    std::vector<InstPlan> ip;
-    std::vector<grp::Inst> host_inst;
-    grp::Inst *d_inst = nullptr;
-    int64_t *d_seg = nullptr;
-    grp::TileRec *d_tiles = nullptr;
-    int32_t *d_cta = nullptr;
+    GroupedTables t;
+    GroupedDevice d;
+    void *dev_tables = nullptr;
     void *ws = nullptr;
     bool owns_ws = false;
-    size_t ws_bytes = 0;
-    int64_t ntiles = 0, nitems = 0;
-    int grid = 0, nseg = 0;
-    double flops = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    int device = 0;
 };
 
 size_t grouped_workspace_bytes(int engine, const gatlas_grouped_instance *in, int32_t count) {
-    if ((engine != GATLAS_ENGINE_TC_BF16 && engine != GATLAS_ENGINE_TC_SPLIT3) || !in || count < 0) return 0;
-    const int np = engine == GATLAS_ENGINE_TC_SPLIT3 ? 2 : 1;
+    if (!grouped_engine_ok(engine) || !in || count < 0) return 0;
     size_t total = 0;
     for (int i = 0; i < count; ++i) {
-        InstPlan o{};
-        if (resolve_instance(in[i], np, engine_slot(engine), &o)) return 0;
-        total += np * (o.a_piece + o.b_piece);
+        size_t b = 0;
+        if (grouped_instance_bytes(engine, in[i], &b)) return 0;
+        total += b;
     }
     return total;
 }
@@ -539,48 +654,64 @@ size_t grouped_workspace_bytes(int engine, const gatlas_grouped_instance *in, in
 static void free_plan(GroupedPlan *p) {
     for (auto &g : p->graph)
         if (g) cudaGraphExecDestroy(g);
-    cudaFree(p->d_inst);
-    cudaFree(p->d_seg);
-    cudaFree(p->d_tiles);
-    cudaFree(p->d_cta);
+    cudaFree(p->dev_tables);
     if (p->owns_ws) cudaFree(p->ws);
     delete p;
+}
+
+// Byte layout of the device tables: [inst][seg][tiles][cta], 256-byte aligned parts.
+static size_t table_layout(const GroupedTables &t, size_t off[4]) {
+    const size_t sz[4] = {t.inst.size() * sizeof(grp::Inst), t.seg.size() * sizeof(int64_t),
+                          t.tiles.size() * sizeof(grp::TileRec), t.cta.size() * sizeof(int32_t)};
+    size_t o = 0;
+    for (int i = 0; i < 4; ++i) {
+        off[i] = o;
+        o += round_up(sz[i], 256);
+    }
+    return o;
+}
+
+size_t grouped_tables_bytes(const GroupedTables &t) {
+    size_t off[4];
+    return table_layout(t, off);
+}
+
+void grouped_tables_serialise(const GroupedTables &t, void *host_dst) {
+    size_t off[4];
+    table_layout(t, off);
+    uint8_t *h = static_cast<uint8_t *>(host_dst);
+    std::memcpy(h + off[0], t.inst.data(), t.inst.size() * sizeof(grp::Inst));
+    std::memcpy(h + off[1], t.seg.data(), t.seg.size() * sizeof(int64_t));
+    std::memcpy(h + off[2], t.tiles.data(), t.tiles.size() * sizeof(grp::TileRec));
+    std::memcpy(h + off[3], t.cta.data(), t.cta.size() * sizeof(int32_t));
+}
+
+GroupedDevice grouped_tables_device(const GroupedTables &t, const void *dev_base) {
+    size_t off[4];
+    table_layout(t, off);
+    const uint8_t *b = static_cast<const uint8_t *>(dev_base);
+    GroupedDevice d;
+    d.inst = reinterpret_cast<const grp::Inst *>(b + off[0]);
+    d.seg = reinterpret_cast<const int64_t *>(b + off[1]);
+    d.tiles = reinterpret_cast<const grp::TileRec *>(b + off[2]);
+    d.cta = reinterpret_cast<const int32_t *>(b + off[3]);
+    return d;
 }
 
 int grouped_create(int engine, const gatlas_grouped_instance *in, int32_t count, void *ws, size_t ws_bytes,
                    GroupedPlan **out) {
     if (!out) return set_error(GATLAS_ERR_INVALID, "grouped: null plan pointer");
     *out = nullptr;
-    if (engine != GATLAS_ENGINE_TC_BF16 && engine != GATLAS_ENGINE_TC_SPLIT3)
-        return set_error(GATLAS_ERR_UNSUPPORTED, "grouped: engine %d has no grouped kernel (tc_bf16, tc_split3)", engine);
-    if (count < 0 || (count > 0 && !in)) return set_error(GATLAS_ERR_INVALID, "grouped: invalid instance list");
     GroupedPlan *p = new GroupedPlan();
-    p->engine = engine;
-    p->np = engine == GATLAS_ENGINE_TC_SPLIT3 ? 2 : 1;
-    p->mode = engine == GATLAS_ENGINE_TC_SPLIT3 ? 1 : 0;
     p->count = count;
-    p->in.assign(in, in + count);
-    p->ip.resize(count);
-    cudaGetDevice(&p->device);
-    size_t total = 0;
-    for (int i = 0; i < count; ++i) {
-        int rc = resolve_instance(in[i], p->np, engine_slot(engine), &p->ip[i]);
-        if (rc) {
-            delete p;
-            return rc;
-        }
-        const gatlas_grouped_instance &q = in[i];
-        if (q.m > 0 && q.n > 0 && (!q.c || (q.k > 0 && (!q.a || !q.b)))) {
-            delete p;
-            return set_error(GATLAS_ERR_INVALID, "grouped: instance %d has a null pointer", i);
-        }
-        if (p->ip[i].mt > 65535 || p->ip[i].kt > (1 << 24)) {
-            delete p;
-            return set_error(GATLAS_ERR_INVALID, "grouped: instance %d is too large", i);
-        }
-        total += p->np * (p->ip[i].a_piece + p->ip[i].b_piece);
-        p->flops += 2.0 * (double)q.m * (double)q.n * (double)q.k;
+    if (count > 0 && in) p->in.assign(in, in + count);
+    // validate and size before any device work
+    int rc = grouped_build(engine, in, count, nullptr, nullptr, &p->t);
+    if (rc) {
+        delete p;
+        return rc;
     }
+    const size_t total = p->t.packed_bytes;
     if (ws) {
         if (ws_bytes < total) {
             delete p;
@@ -599,141 +730,33 @@ int grouped_create(int engine, const gatlas_grouped_instance *in, int32_t count,
         }
         p->owns_ws = true;
     }
-    p->ws_bytes = total;
-
-    // instance records, pack segments and output tiles
-    p->host_inst.resize(std::max(count, 1));
-    std::vector<int64_t> seg(2 * (size_t)count + 1, 0);
-    struct Cand {
-        int64_t cost;
-        grp::TileRec t;
-    };
-    std::vector<Cand> tiles;
-    uint8_t *base = static_cast<uint8_t *>(p->ws);
-    size_t off = 0;
-    for (int i = 0; i < count; ++i) {
-        const InstPlan &o = p->ip[i];
-        const gatlas_grouped_instance &q = in[i];
-        grp::Inst &I = p->host_inst[i];
-        std::memset(&I, 0, sizeof(I));
-        I.src_a = q.a;
-        I.src_b = q.b;
-        for (int j = 0; j < p->np; ++j) {
-            I.pa[j] = base + off + j * o.a_piece;
-            I.pb[j] = base + off + p->np * o.a_piece + j * o.b_piece;
-        }
-        off += p->np * (o.a_piece + o.b_piece);
-        I.C = q.c;
-        I.M = o.M, I.N = o.N, I.K = o.K, I.lda = o.lda, I.ldb = o.ldb, I.ldc = o.ldc;
-        I.ta = q.trans_a != 0, I.tb = q.trans_b != 0, I.gemm = q.gemm != 0;
-        I.bn = o.bn, I.mt = o.mt, I.nt = o.nt, I.kt = o.kt;
-        I.alpha = (float)q.alpha;
-        I.beta = (float)q.beta;
-        const int64_t a_items = o.kt ? (int64_t)o.mt * o.kt : 0;  // 128 A rows per item = one A tile row block
-        const int64_t b_items = o.kt ? ((int64_t)o.nt * o.bn + grp::kPackRows - 1) / grp::kPackRows * o.kt : 0;
-        seg[2 * i + 1] = seg[2 * i] + a_items;
-        seg[2 * i + 2] = seg[2 * i + 1] + b_items;
-        // cost in bytes moved: operand tiles through shared memory plus the C
-        // tile (read too when beta != 0), plus a fixed per-tile overhead
-        const int64_t c_bytes = (int64_t)grp::BM * o.bn * 4 * ((q.gemm && q.beta != 0.0) ? 2 : 1);
-        const int64_t cost = (int64_t)o.kt * p->np * (grp::BM + o.bn) * grp::kRowBytes + c_bytes + 16384;
-        for (int tm = 0; tm < o.mt; ++tm)
-            for (int tn = 0; tn < o.nt; ++tn) {
-                grp::TileRec r;
-                std::memset(&r, 0, sizeof(r));
-                for (int j = 0; j < p->np; ++j) {
-                    r.a[j] = I.pa[j] + (size_t)tm * o.kt * grp::kATileBytes;
-                    r.b[j] = I.pb[j] + (size_t)tn * o.kt * o.bn * grp::kRowBytes;
-                }
-                r.C = q.c + (int64_t)tm * grp::BM * o.ldc + (int64_t)tn * o.bn;
-                r.ldc = o.ldc;
-                r.kt = o.kt;
-                r.bn = o.bn;
-                r.rows = (int32_t)std::min<int64_t>(grp::BM, o.M - (int64_t)tm * grp::BM);
-                r.cols = (int32_t)std::min<int64_t>(o.bn, o.N - (int64_t)tn * o.bn);
-                r.alpha = (float)q.alpha;
-                r.beta = (float)q.beta;
-                r.gemm = q.gemm != 0;
-                tiles.push_back(Cand{cost, r});
-            }
+    rc = grouped_build(engine, in, count, static_cast<uint8_t *>(p->ws), nullptr, &p->t);
+    if (rc) {
+        free_plan(p);
+        return rc;
     }
-    p->nseg = 2 * count;
-    p->nitems = seg.back();
-    p->ntiles = (int64_t)tiles.size();
-    // longest first onto the least-loaded CTA
-    std::stable_sort(tiles.begin(), tiles.end(), [](const Cand &a, const Cand &b) { return a.cost > b.cost; });
-    p->grid = (int)std::min<int64_t>(sm_count(), std::max<int64_t>(p->ntiles, 1));
-    std::vector<std::vector<grp::TileRec>> per(p->grid);
-    {
-        using E = std::pair<int64_t, int>;
-        std::priority_queue<E, std::vector<E>, std::greater<E>> heap;
-        for (int b = 0; b < p->grid; ++b) heap.push({0, b});
-        for (const Cand &c : tiles) {
-            E e = heap.top();
-            heap.pop();
-            per[e.second].push_back(c.t);
-            heap.push({e.first + c.cost, e.second});
-        }
-    }
-    std::vector<grp::TileRec> flat;
-    std::vector<int32_t> cta(p->grid + 1, 0);
-    flat.reserve(tiles.size());
-    for (int b = 0; b < p->grid; ++b) {
-        cta[b] = (int32_t)flat.size();
-        flat.insert(flat.end(), per[b].begin(), per[b].end());
-    }
-    cta[p->grid] = (int32_t)flat.size();
-    if (flat.empty()) flat.push_back(grp::TileRec{});
-    bool ok = cudaMalloc(&p->d_inst, p->host_inst.size() * sizeof(grp::Inst)) == cudaSuccess &&
-              cudaMalloc(&p->d_seg, seg.size() * sizeof(int64_t)) == cudaSuccess &&
-              cudaMalloc(&p->d_tiles, flat.size() * sizeof(grp::TileRec)) == cudaSuccess &&
-              cudaMalloc(&p->d_cta, cta.size() * sizeof(int32_t)) == cudaSuccess;
-    ok = ok && cudaMemcpy(p->d_inst, p->host_inst.data(), p->host_inst.size() * sizeof(grp::Inst),
-                          cudaMemcpyHostToDevice) == cudaSuccess;
-    ok = ok && cudaMemcpy(p->d_seg, seg.data(), seg.size() * sizeof(int64_t), cudaMemcpyHostToDevice) == cudaSuccess;
-    ok = ok && cudaMemcpy(p->d_tiles, flat.data(), flat.size() * sizeof(grp::TileRec), cudaMemcpyHostToDevice) ==
-                   cudaSuccess;
-    ok = ok && cudaMemcpy(p->d_cta, cta.data(), cta.size() * sizeof(int32_t), cudaMemcpyHostToDevice) == cudaSuccess;
-    if (!ok) {
+    const size_t tb = grouped_tables_bytes(p->t);
+    std::vector<uint8_t> host(tb);
+    grouped_tables_serialise(p->t, host.data());
+    if (cudaMalloc(&p->dev_tables, tb) != cudaSuccess ||
+        cudaMemcpy(p->dev_tables, host.data(), tb, cudaMemcpyHostToDevice) != cudaSuccess) {
         cudaGetLastError();
         free_plan(p);
         return set_error(GATLAS_ERR_NOMEM, "grouped: device tables");
     }
+    p->d = grouped_tables_device(p->t, p->dev_tables);
     *out = p;
     return GATLAS_OK;
 }
 
 int grouped_prepare(GroupedPlan *p, cudaStream_t stream) {
     if (!p) return set_error(GATLAS_ERR_INVALID, "grouped: null plan");
-    if (p->nitems == 0) return GATLAS_OK;
-    const int64_t grid = std::min<int64_t>(p->nitems, (int64_t)sm_count() * 8);
-    const int64_t per_cta = (p->nitems + grid - 1) / grid;
-    if (p->np == 2)
-        grp::grouped_pack_kernel<2><<<(unsigned)grid, 256, 0, stream>>>(p->d_inst, p->d_seg, p->nseg, per_cta);
-    else
-        grp::grouped_pack_kernel<1><<<(unsigned)grid, 256, 0, stream>>>(p->d_inst, p->d_seg, p->nseg, per_cta);
-    return check_launch("grouped_pack_kernel");
-}
-
-template <int MODE>
-static int launch_grouped(GroupedPlan *p, int seg_kblocks, cudaStream_t stream) {
-    using L = tcg::Layout<MODE>;
-    grp::Params prm;
-    prm.tiles = p->d_tiles;
-    prm.cta_start = p->d_cta;
-    prm.seg_kblocks = seg_kblocks > 0 ? seg_kblocks : tcg::kDefaultSegKblocks;
-    prm.fault = device_fault_word();
-    const int smem = (int)L::SMEM_BYTES;
-    cudaError_t e = cudaFuncSetAttribute(grp::grouped_gemm_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "grouped smem attribute: %s", cudaGetErrorString(e));
-    grp::grouped_gemm_kernel<MODE><<<p->grid, grp::kThreads, smem, stream>>>(prm);
-    return check_launch("grouped_gemm_kernel");
+    return grouped_launch_pack(p->t, p->d, stream);
 }
 
 int grouped_run(GroupedPlan *p, cudaStream_t stream) {
     if (!p) return set_error(GATLAS_ERR_INVALID, "grouped: null plan");
-    if (p->ntiles == 0) return GATLAS_OK;
-    return p->mode == 1 ? launch_grouped<1>(p, 0, stream) : launch_grouped<0>(p, 0, stream);
+    return grouped_launch_contract(p->t, p->d, stream);
 }
 
 int grouped_launch_graph(GroupedPlan *p, int with_prepare, cudaStream_t stream) {
@@ -779,12 +802,12 @@ static gatlas_matmul_desc instance_desc(const GroupedPlan *p, int i) {
     const gatlas_grouped_instance &q = p->in[i];
     gatlas_matmul_desc d;
     std::memset(&d, 0, sizeof(d));
-    d.engine = p->engine;
+    d.engine = p->t.engine;
     d.gemm = q.gemm;
     d.trans_a = q.trans_a;
     d.trans_b = q.trans_b;
     d.m = q.m, d.n = q.n, d.k = q.k;
-    d.lda = p->ip[i].lda, d.ldb = p->ip[i].ldb, d.ldc = p->ip[i].ldc;
+    d.lda = p->t.ip[i].lda, d.ldb = p->t.ip[i].ldb, d.ldc = p->t.ip[i].ldc;
     d.batch = 1;
     d.alpha = q.alpha;
     d.beta = q.beta;
@@ -813,10 +836,10 @@ int grouped_run_each(GroupedPlan *p, cudaStream_t stream) {
 
 int grouped_info(const GroupedPlan *p, int64_t *tiles, int32_t *ctas, double *flops, int64_t *items) {
     if (!p) return set_error(GATLAS_ERR_INVALID, "grouped: null plan");
-    if (tiles) *tiles = p->ntiles;
-    if (ctas) *ctas = p->grid;
-    if (flops) *flops = p->flops;
-    if (items) *items = p->nitems;
+    if (tiles) *tiles = p->t.ntiles;
+    if (ctas) *ctas = p->t.grid;
+    if (flops) *flops = p->t.flops;
+    if (items) *items = p->t.nitems;
     return GATLAS_OK;
 }
 

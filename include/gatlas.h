@@ -228,6 +228,70 @@ int gatlas_grouped_get_tile_table(int engine, int32_t *bucket_tile_n, int32_t nb
 int gatlas_grouped_autotune(int engine, const char *journal_path, int32_t trials, uint64_t seed,
                             int32_t *out_table);
 
+/* ---- serving ---------------------------------------------------------------
+ * A request loop over mixed GEMM / GEMV / SAXPY solves (no reference
+ * counterpart: the reference times one kernel at a time).  A trace of
+ * requests with arrival times is replayed in real time.  Continuous mode:
+ * FIFO admission into a device arena of budget_bytes (a request that does
+ * not fit waits, and later arrivals do not overtake it), operands generated
+ * from each request's seed on a prep stream, every admitted GEMM batched
+ * into one grouped tensor-core launch whenever fewer than two GEMM batches
+ * are on the device (at most max_batch GEMMs, or about batch_target_ms of
+ * estimated work), GEMVs and SAXPYs launched as admitted on a second
+ * stream.  Serial mode: one request at a time, one engine call each,
+ * synchronised.  Results of the same request are bit-identical in both modes
+ * and alone or in any mix. */
+enum { GATLAS_REQ_GEMM = 0, GATLAS_REQ_GEMV = 1, GATLAS_REQ_SAXPY = 2 };
+enum { GATLAS_SERVE_CONTINUOUS = 0, GATLAS_SERVE_SERIAL = 1 };
+
+typedef struct gatlas_request {
+    int32_t kind;             /* GATLAS_REQ_* */
+    int32_t trans_a, trans_b; /* GEMM layouts; GEMV: trans_a = column-major A */
+    int32_t retain;           /* keep the result (and the request's memory) until gatlas_server_release */
+    int64_t m, n, k;          /* GEMM m x n x k; GEMV A m x n (y = alpha*A*x + beta*y); SAXPY length n */
+    double alpha, beta;       /* GEMM C = alpha*op(A)op(B) + beta*C; SAXPY y = alpha*x + y */
+    uint64_t seed;            /* operands: uniform[-1,1) streams 4*seed, 4*seed+1, 4*seed+2 (initial result) */
+    int64_t arrival_ns;       /* from the start of the run, non-decreasing */
+} gatlas_request;
+
+typedef struct gatlas_request_result {
+    int64_t admit_ns, start_ns, done_ns; /* from the start of the run; done on the device timeline */
+    int32_t status;                      /* GATLAS_OK or the request's error */
+    int32_t batch;                       /* GEMM batch index, -1 for single launches */
+    float *result;                       /* retained device result (C, y), else NULL */
+    int64_t result_elems;
+} gatlas_request_result;
+
+typedef struct gatlas_server_config {
+    size_t budget_bytes;         /* device-memory admission budget (one arena) */
+    int32_t gemm_engine;         /* GATLAS_ENGINE_TC_SPLIT3 or GATLAS_ENGINE_TC_BF16 */
+    int32_t max_batch;           /* most GEMMs per grouped launch (0: 256) */
+    double batch_target_ms;      /* estimated device time per GEMM batch (0: 20 ms) */
+    double gemm_tflops_estimate; /* rate behind that estimate, FP32-equivalent TFLOP/s (0: 300) */
+} gatlas_server_config;
+
+typedef struct gatlas_server_stats_t {
+    size_t budget_bytes, peak_bytes, used_bytes;
+    int64_t gemm_batches, batched_gemms;
+    int64_t host_busy_ns; /* host time spent in loop iterations that did work */
+    int64_t iterations;   /* loop iterations */
+    /* host ns per phase: harvest, admission (incl. operand generation),
+     * single launches, GEMM batch tables, GEMM batch launches */
+    int64_t phase_ns[5];
+} gatlas_server_stats_t;
+
+typedef struct gatlas_server gatlas_server;
+
+int gatlas_server_create(const gatlas_server_config *cfg, gatlas_server **srv);
+/* Blocks until every request is done; results[i] belongs to reqs[i]. */
+int gatlas_server_run(gatlas_server *srv, const gatlas_request *reqs, int32_t count, int32_t mode,
+                      gatlas_request_result *results);
+int gatlas_server_release(gatlas_server *srv, float *result);
+/* Copies elems floats of a retained result to host memory (synchronous). */
+int gatlas_server_read(gatlas_server *srv, const float *result, float *host_dst, int64_t elems);
+int gatlas_server_stats(const gatlas_server *srv, gatlas_server_stats_t *out);
+void gatlas_server_destroy(gatlas_server *srv);
+
 /* ---- data generation and residuals ---------------------------------------
  * Seeded device-side generators (splitmix64 counter streams shared with the
  * host oracle): uniform [-1,1), sign·2^e (e in [-8,8]) or a constant. */
