@@ -178,6 +178,42 @@ def _timed(fn, steps, warmup, world, stream):
     return start.elapsed_time(stop) / steps  # ms per step
 
 
+SGEMM_TUNE_N = 1024
+SGEMM_TUNE_GRID = [(gh, gw, bh, bw, vl) for gh in (8, 16) for gw in (8, 16) for bh in (4, 8) for bw in (4, 8)
+                   for vl in (1, 2, 4)]
+
+
+def sgemm_autotune_leg(world, stream):
+    """Plain SGEMM 1024^3 (alpha 1, beta 0, row-major, no transposes) on the
+    SIMT engine, autotuned over work group {8,16}^2 x inner blocking {4,8}^2 x
+    vector width {1,2,4}; the winner is checked against the FP64 product."""
+    import torch
+
+    import gatlas_b200 as g
+    dev = torch.cuda.current_device()
+    n = SGEMM_TUNE_N
+    A = torch.empty(n * n, device=dev)
+    B = torch.empty(n * n, device=dev)
+    C = torch.empty(n * n, device=dev)
+    g.fill(A, "uniform", seed=1)
+    g.fill(B, "uniform", seed=2)
+    times = {}
+    for pt in SGEMM_TUNE_GRID:
+        tile = pt + (0,)
+        times[pt] = _timed(lambda: g.matmul(A, B, n, n, n, C=C, tile=tile), 10, 3, world, stream)
+    best = min(times, key=times.get)
+    g.matmul(A, B, n, n, n, C=C, tile=best + (0,))
+    fro, ref, mx, _ = g.residual(A, B, C, n, n, n)
+    flops = 2.0 * n ** 3
+    ranked = sorted(times.items(), key=lambda kv: kv[1])
+    return {"m": n, "n": n, "k": n, "points": len(times), "best_tile": dict(zip(("gh", "gw", "bh", "bw", "vl"), best)),
+            "best_ms": times[best], "best_tflops": flops / (times[best] * 1e-3) / 1e12,
+            "reference_flops": float(n * n * (2 * n - 1)),
+            "worst_tflops": flops / (ranked[-1][1] * 1e-3) / 1e12,
+            "top5": [{"tile": list(k), "tflops": flops / (v * 1e-3) / 1e12} for k, v in ranked[:5]],
+            "error_vs_fp64": {"normwise": fro / ref, "max_abs": mx}}
+
+
 GROUPED_INSTANCES = 1024
 
 
@@ -486,6 +522,9 @@ def run_ours(args, rank, world, local):
     secondary["hbm_peak_gbs"] = peaks["hbm_gbs"]
     del xs, ys
 
+    # ---- plain SGEMM 1024^3, autotuned SIMT point ---------------------------------
+    sgemm_1024 = sgemm_autotune_leg(world, stream)
+
     # ---- batched uneven GEMM (grouped persistent kernel) ------------------------
     grouped = grouped_leg(args, world, stream) if not args.quick else None
 
@@ -508,7 +547,7 @@ def run_ours(args, rank, world, local):
                    "l2": "operands larger than L2; no flush"},
         "error_vs_fp64": {"normwise": fro / refn, "max_abs": mx},
         "e2e": e2e, "roofline": roofline, "precision_sweep": sweep, "secondary": secondary,
-        "grouped": grouped, "serving": serving,
+        "sgemm_1024_autotune": sgemm_1024, "grouped": grouped, "serving": serving,
         "gpu_launches": launches_per_step * args.steps, "clocks": clocks,
         "device_faults": faults,
     }

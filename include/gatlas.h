@@ -130,7 +130,13 @@ int gatlas_matvec_f32_noalloc(const gatlas_matvec_desc *d, const float *A, const
  * element, bit-exact against a sequential fmaf chain.  For the TC_* engines
  * the tile fields are ignored and `extra` is the promotion interval: the
  * tensor cores accumulate `extra` slices of K = 32 in TMEM before the partial
- * sum is added into round-to-nearest FP32 registers (0 selects 4, K = 128). */
+ * sum is added into round-to-nearest FP32 registers (0 selects 4, K = 128).
+ * GATLAS_ENGINE_TC_FP8 quantises each operand to E4M3 with one power-of-two
+ * FP32 scale per 128 x 128 block (the smallest power of two s with
+ * amax / s <= 448) and promotes every 128-deep block scaled by sa * sb; its
+ * tc_prepare workspace holds [A codes][B codes][A scales][B scales], codes
+ * K-major [batch][rows][Kp] (Kp = K rounded up to 16), scales
+ * [batch][rows/128][K/128], each part 1024-byte aligned. */
 typedef struct gatlas_matmul_desc {
     int32_t engine;
     int32_t gemm;
@@ -314,7 +320,7 @@ int gatlas_matmul_residual_f32(const gatlas_matmul_desc *d, const float *A, cons
  * (KernelInterface, GatlasBenchmark.hpp:28-58; KernelBase{Matmul,Matvec,
  * Saxpy}).  op is "matmul", "matvec" or "saxpy"; type is a -T name of the
  * reference's tools (float1|float2|float4|double1|double2|double4|floatimg|
- * doubleimg), or tcbf16|split3|split6 for the tensor-core matmul engines.
+ * doubleimg), or tcbf16|split3|split6|fp8 for the tensor-core matmul engines.
  * String and vector getters return the full length and copy at most
  * len - 1 characters / cap elements. */
 typedef struct gatlas_kernel gatlas_kernel;
