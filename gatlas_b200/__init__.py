@@ -113,6 +113,8 @@ def lib() -> ctypes.CDLL:
     L.gatlas_matmul_residual_f32.argtypes = [ctypes.POINTER(MatmulDesc), vp, vp, vp,
                                              ctypes.POINTER(ctypes.c_double), vp]
     L.gatlas_device_faults.argtypes = [ctypes.POINTER(ctypes.c_int), i32]
+    L.gatlas_set_option.argtypes = [ctypes.c_char_p, ctypes.c_int64]
+    L.gatlas_get_option.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
     gi = ctypes.POINTER(GroupedInstance)
     L.gatlas_grouped_workspace_size.argtypes = [i32, gi, ctypes.c_int32]
     L.gatlas_grouped_workspace_size.restype = sz
@@ -489,3 +491,14 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def set_option(name: str, value: int) -> None:
+    """Library options (see gatlas_set_option): "tc_pair"."""
+    check(lib().gatlas_set_option(name.encode(), int(value)))
+
+
+def get_option(name: str) -> int:
+    v = ctypes.c_int64()
+    check(lib().gatlas_get_option(name.encode(), ctypes.byref(v)))
+    return int(v.value)

@@ -130,7 +130,7 @@ __device__ __forceinline__ void bulk_wait() {
     asm volatile("cp.async.bulk.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// 2-D tiled tensor copy global -> shared (no multicast).  x is the innermost
+// 2-D tiled tensor copy global -> this CTA's shared memory.  x is the innermost
 // coordinate; the caller keeps x * element size a multiple of 16 bytes.
 __device__ __forceinline__ void tma_load_2d(void *smem_dst, const void *tmap, int32_t x, int32_t y,
                                             uint64_t *bar) {

@@ -23,6 +23,8 @@
 // Every mbarrier wait is bounded in wall time; a timeout sets the device
 // fault word, stops the pipeline, drains the copies in flight and frees TMEM.
 #include <cuda.h>
+
+#include <cstring>
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
 
@@ -51,6 +53,7 @@ struct Params {
     const float *scale_a, *scale_b;
     int64_t scale_a_stride, scale_b_stride;  // per instance
     int nblocks_n;                           // 128-column blocks of N
+    int nblocks_m;                           // 128-row blocks of M
 };
 
 // Warp roles: warp 0 = TMA producer (lane 0), warp 1 = MMA issuer (lane 0),
@@ -95,7 +98,7 @@ __global__ void __launch_bounds__(kThreads2, 1)
     constexpr int BK = L::BK;
     const CUtensorMap *tA[3] = {&ta0, &ta1, &ta2};
     const CUtensorMap *tB[3] = {&tb0, &tb1, &tb2};
-    const int nseg = (p.kblocks + p.seg_kblocks - 1) / p.seg_kblocks;
+    __shared__ int fp8_nseg;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; ++s) {
@@ -123,6 +126,52 @@ __global__ void __launch_bounds__(kThreads2, 1)
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = tmem_base;
+
+    // Segment plan.  BF16 modes: fixed runs of seg_kblocks slices.  FP8: a
+    // segment is a run of at most seg_kblocks 128-deep blocks whose scale
+    // products sa*sb are equal for both column halves of the tile; the
+    // tensor core accumulates the run in TMEM and the drain scales it once,
+    // which is exact because the scales are powers of two.
+    float *seg_q0 = nullptr, *seg_q1 = nullptr;
+    uint8_t *seg_flag = nullptr;
+    int nseg = (p.kblocks + p.seg_kblocks - 1) / p.seg_kblocks;
+    if constexpr (MD::SCALED) {
+        seg_q0 = reinterpret_cast<float *>(smem + S * L::STAGE_BYTES);
+        seg_q1 = seg_q0 + kMaxFp8Blocks;
+        seg_flag = reinterpret_cast<uint8_t *>(seg_q1 + kMaxFp8Blocks);
+        const int nb0 = tile_n * 2;
+        const float *sa = p.scale_a + z * p.scale_a_stride + (int64_t)tile_m * p.kblocks;
+        const float *sb0 = nb0 < p.nblocks_n ? p.scale_b + z * p.scale_b_stride + (int64_t)nb0 * p.kblocks : nullptr;
+        const float *sb1 =
+            nb0 + 1 < p.nblocks_n ? p.scale_b + z * p.scale_b_stride + (int64_t)(nb0 + 1) * p.kblocks : nullptr;
+        for (int kb = threadIdx.x; kb < p.kblocks; kb += blockDim.x) {
+            const float a = sa[kb];
+            seg_q0[kb] = sb0 ? __fmul_rn(a, sb0[kb]) : 0.0f;
+            seg_q1[kb] = sb1 ? __fmul_rn(a, sb1[kb]) : 0.0f;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int s = -1, run = 0;
+            float prev0 = 0.0f, prev1 = 0.0f;
+            for (int kb = 0; kb < p.kblocks; ++kb) {
+                const float q0 = seg_q0[kb], q1 = seg_q1[kb];
+                const bool start = kb == 0 || run == p.seg_kblocks || q0 != prev0 || q1 != prev1;
+                if (start) {
+                    ++s;
+                    run = 0;
+                    seg_q0[s] = q0;  // s <= kb: compacted in place
+                    seg_q1[s] = q1;
+                }
+                seg_flag[kb] = start ? 1 : 0;
+                ++run;
+                prev0 = q0;
+                prev1 = q1;
+            }
+            fp8_nseg = s + 1;
+        }
+        __syncthreads();
+        nseg = fp8_nseg;
+    }
 
     auto a_tile = [&](int s, int piece) { return smem + s * L::STAGE_BYTES + piece * L::A_TILE; };
     auto b_tile = [&](int s, int piece) { return smem + s * L::STAGE_BYTES + MD::NP * L::A_TILE + piece * L::B_TILE; };
@@ -152,11 +201,18 @@ __global__ void __launch_bounds__(kThreads2, 1)
         if (lane == 0) {
             // ---- MMA issuer: segment g accumulates into TMEM buffer g & 1 ----
             constexpr uint32_t idesc = L::IDESC;
-            int kb = 0;
+            int kb = 0, seg = -1;
             for (; kb < p.kblocks; ++kb) {
-                const int seg = kb / p.seg_kblocks, b = seg & 1;
-                const bool seg_first = (kb % p.seg_kblocks) == 0;
-                const bool seg_last = (kb % p.seg_kblocks) == p.seg_kblocks - 1 || kb == p.kblocks - 1;
+                bool seg_first, seg_last;
+                if constexpr (MD::SCALED) {
+                    seg_first = seg_flag[kb] != 0;
+                    seg_last = kb == p.kblocks - 1 || seg_flag[kb + 1] != 0;
+                } else {
+                    seg_first = (kb % p.seg_kblocks) == 0;
+                    seg_last = (kb % p.seg_kblocks) == p.seg_kblocks - 1 || kb == p.kblocks - 1;
+                }
+                if (seg_first) ++seg;
+                const int b = seg & 1;
                 if (seg_first) {
                     // the drain of this buffer's previous segment must be done
                     if (!tc::wait_timed(&tempty[b], ((uint32_t)(seg >> 1) & 1u) ^ 1u, kWaitNs, &abort_flag)) {
@@ -207,19 +263,10 @@ __global__ void __launch_bounds__(kThreads2, 1)
 #pragma unroll
         for (int j = 0; j < BN / 2; ++j) acc[j] = 0.0f;
         bool ok = true;
-        // FP8: this warp's column half is one 128-column scale block of B
-        const int nblk = tile_n * 2 + half;
-        const float *sa_row = MD::SCALED ? p.scale_a + z * p.scale_a_stride + (int64_t)tile_m * p.kblocks : nullptr;
-        const float *sb_row = (MD::SCALED && nblk < p.nblocks_n)
-                                  ? p.scale_b + z * p.scale_b_stride + (int64_t)nblk * p.kblocks
-                                  : nullptr;
         for (int seg = 0; seg < nseg; ++seg) {
             const int b = seg & 1;
             float scale = 1.0f;
-            if constexpr (MD::SCALED) {
-                // loaded before the wait, so the latency hides behind it
-                scale = sb_row ? __fmul_rn(__ldg(sa_row + seg), __ldg(sb_row + seg)) : 0.0f;
-            }
+            if constexpr (MD::SCALED) scale = half ? seg_q1[seg] : seg_q0[seg];  // this half's scale block
             if (!tc::wait_timed(&tfull[b], (uint32_t)(seg >> 1) & 1u, 2 * kWaitNs, &abort_flag)) {
                 if (!abort_flag) report_fault(p.fault, kFaultTcEpilogueWait);
                 abort_flag = 1;
@@ -286,6 +333,324 @@ __global__ void __launch_bounds__(kThreads2, 1)
     }
     __syncthreads();
     if (warp == 0) tc::tmem_dealloc(tmem, kTmemCols2);
+}
+
+// ---------------------------------------------------------------------------
+// CTA-pair contraction (cta_group::2): one 256 x 256 tile per cluster of two
+// ---------------------------------------------------------------------------
+// Each CTA streams 128 rows of A and its 128-row half of B per K slice
+// (instead of 128 + 256 rows for a 128 x 256 tile), so the operand bytes
+// moved from L2 per FLOP fall by a third and the ring gets deeper for the
+// same shared memory.  Roles per CTA as in tc_gemm_kernel; only the leader
+// (rank 0) issues MMAs, M = 256 split by rows across the two TMEMs.
+// Barriers (no multicast forms anywhere):
+//  * full[s] of the leader: both producers' TMA loads complete on it; the
+//    leader's producer arrives once with the pair's byte count;
+//  * empty[s] and tfull[b] of each CTA: the leader's MMA commits to its own
+//    barrier and to the peer's;
+//  * tempty[b] of the leader: 16 arrivals, the 8 drain warps of each CTA.
+// Every wait is bounded; after an abort each CTA lets in-flight copies land
+// before the closing cluster barrier, so neither CTA leaves while the pair's
+// MMAs or copies can still touch its shared memory.
+template <int MODE>
+__global__ void __launch_bounds__(kThreads2, 1)
+    tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap ta0, const __grid_constant__ CUtensorMap ta1,
+                        const __grid_constant__ CUtensorMap ta2, const __grid_constant__ CUtensorMap tb0,
+                        const __grid_constant__ CUtensorMap tb1, const __grid_constant__ CUtensorMap tb2,
+                        Params p) {
+    using L = PairLayout<MODE>;
+    using MD = Mode<MODE>;
+    constexpr int S = L::STAGES;
+    constexpr int BK = L::BK;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    __shared__ __align__(8) uint64_t full[S], empty[S], tfull[2], tempty[2], mma_done;
+    __shared__ uint32_t tmem_base;
+    __shared__ volatile int abort_flag;
+    __shared__ int kb_issued, kb_consumed, mma_aborted, fp8_nseg;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = tc::cluster_ctarank();
+    const bool leader = rank == 0;
+    int tile_m, tile_n;  // in pair tiles (256 x 256)
+    {
+        const int tiles_n = (int)((p.N + L::PN - 1) / L::PN), tiles_m = (int)((p.M + L::PM - 1) / L::PM);
+        const int bid = (int)(blockIdx.x >> 1);
+        const int per_group = kGroupM * tiles_n;
+        const int first_m = (bid / per_group) * kGroupM;
+        const int gm = min(tiles_m - first_m, kGroupM);
+        const int r = bid % per_group;
+        tile_m = first_m + r % gm;
+        tile_n = r / gm;
+    }
+    const int m0 = tile_m * L::PM + (int)rank * 128;  // this CTA's rows of A and C
+    const int n0 = tile_n * L::PN;                    // the pair's columns
+    const int nb = n0 + (int)rank * 128;              // this CTA's half of B
+    const int z = blockIdx.z;
+    const CUtensorMap *tA[3] = {&ta0, &ta1, &ta2};
+    const CUtensorMap *tB[3] = {&tb0, &tb1, &tb2};
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], 2 * kDrainWarps);
+        }
+        mbar_init(&mma_done, 1);
+        fence_mbarrier_init();
+        abort_flag = 0;
+        kb_issued = kb_consumed = 0;
+        mma_aborted = 0;
+        for (int i = 0; i < MD::NP; ++i) {
+            prefetch_tmap(tA[i]);
+            prefetch_tmap(tB[i]);
+        }
+    }
+    if (warp == 0) {
+        tc::tmem_alloc_pair(&tmem_base, kTmemCols2);
+        tc::tmem_relinquish_pair();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::cluster_sync();  // both CTAs' barriers exist before any signal crosses the pair
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_base;
+
+    // Segment plan, identical in both CTAs (the leader's MMA serves both).
+    // FP8: a run of at most seg_kblocks blocks whose four scale products (the
+    // pair's two row blocks x two column halves) are all unchanged; each CTA
+    // keeps the segment scales of its own row block.
+    float *seg_q0 = nullptr, *seg_q1 = nullptr;
+    uint8_t *seg_flag = nullptr;
+    int nseg = (p.kblocks + p.seg_kblocks - 1) / p.seg_kblocks;
+    if constexpr (MD::SCALED) {
+        seg_q0 = reinterpret_cast<float *>(smem + S * L::STAGE_BYTES);
+        seg_q1 = seg_q0 + kMaxFp8Blocks;
+        seg_flag = reinterpret_cast<uint8_t *>(seg_q1 + kMaxFp8Blocks);
+        const float *sa[2], *sb[2];
+        for (int i = 0; i < 2; ++i) {
+            const int mb = tile_m * 2 + i, nbk = tile_n * 2 + i;
+            sa[i] = mb < p.nblocks_m ? p.scale_a + z * p.scale_a_stride + (int64_t)mb * p.kblocks : nullptr;
+            sb[i] = nbk < p.nblocks_n ? p.scale_b + z * p.scale_b_stride + (int64_t)nbk * p.kblocks : nullptr;
+        }
+        // per block: change flag of the four products, and this row block's two products
+        for (int kb = threadIdx.x; kb < p.kblocks; kb += blockDim.x) {
+            float q[2][2];
+            for (int i = 0; i < 2; ++i)
+                for (int h = 0; h < 2; ++h) q[i][h] = (sa[i] && sb[h]) ? __fmul_rn(sa[i][kb], sb[h][kb]) : 0.0f;
+            bool change = kb == 0;
+            if (kb > 0)
+                for (int i = 0; i < 2; ++i)
+                    for (int h = 0; h < 2; ++h) {
+                        const float prev = (sa[i] && sb[h]) ? __fmul_rn(sa[i][kb - 1], sb[h][kb - 1]) : 0.0f;
+                        change = change || prev != q[i][h];
+                    }
+            seg_q0[kb] = q[rank][0];
+            seg_q1[kb] = q[rank][1];
+            seg_flag[kb] = change ? 1 : 0;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int s = -1, run = 0;
+            for (int kb = 0; kb < p.kblocks; ++kb) {
+                const bool start = seg_flag[kb] != 0 || run == p.seg_kblocks;
+                if (start) {
+                    ++s;
+                    run = 0;
+                    seg_q0[s] = seg_q0[kb];  // s <= kb: compacted in place
+                    seg_q1[s] = seg_q1[kb];
+                }
+                seg_flag[kb] = start ? 1 : 0;
+                ++run;
+            }
+            fp8_nseg = s + 1;
+        }
+        __syncthreads();
+        nseg = fp8_nseg;
+    }
+
+    auto a_tile = [&](int s, int piece) { return smem + s * L::STAGE_BYTES + piece * L::A_TILE; };
+    auto b_tile = [&](int s, int piece) { return smem + s * L::STAGE_BYTES + MD::NP * L::A_TILE + piece * L::B_TILE; };
+    const uint32_t full_leader = tc::mapa_shared(smem_u32(&full[0]), 0);
+    const uint32_t tempty_leader = tc::mapa_shared(smem_u32(&tempty[0]), 0);
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---- TMA producer (both CTAs): completion counts on the leader's full[s] ----
+            int kb = 0;
+            for (; kb < p.kblocks; ++kb) {
+                const int s = kb % S;
+                const uint32_t ph = (uint32_t)(kb / S) & 1u;
+                if (!tc::wait_timed_cluster(&empty[s], ph ^ 1u, kWaitNs, &abort_flag)) {
+                    if (!abort_flag) report_fault(p.fault, kFaultTcProducerWait);
+                    abort_flag = 1;
+                    break;
+                }
+                if (leader) mbar_arrive_expect_tx(&full[s], 2 * L::STAGE_BYTES);
+                const uint32_t bar = full_leader + (uint32_t)(s * sizeof(uint64_t));
+                for (int i = 0; i < MD::NP; ++i) {
+                    tc::tma_load_3d_pair(a_tile(s, i), tA[i], kb * BK, m0, z, bar);
+                    tc::tma_load_3d_pair(b_tile(s, i), tB[i], kb * BK, nb, z, bar);
+                }
+            }
+            kb_issued = kb;
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0 && leader) {
+            // ---- MMA issuer (leader only) ----
+            constexpr uint32_t idesc = L::IDESC;
+            const uint32_t empty_self = tc::mapa_shared(smem_u32(&empty[0]), 0);
+            const uint32_t empty_peer = tc::mapa_shared(smem_u32(&empty[0]), 1);
+            const uint32_t tfull_self = tc::mapa_shared(smem_u32(&tfull[0]), 0);
+            const uint32_t tfull_peer = tc::mapa_shared(smem_u32(&tfull[0]), 1);
+            int kb = 0, seg = -1;
+            bool stop = false;
+            for (; kb < p.kblocks; ++kb) {
+                bool seg_first, seg_last;
+                if constexpr (MD::SCALED) {
+                    seg_first = seg_flag[kb] != 0;
+                    seg_last = kb == p.kblocks - 1 || seg_flag[kb + 1] != 0;
+                } else {
+                    seg_first = (kb % p.seg_kblocks) == 0;
+                    seg_last = (kb % p.seg_kblocks) == p.seg_kblocks - 1 || kb == p.kblocks - 1;
+                }
+                if (seg_first) ++seg;
+                const int b = seg & 1;
+                if (seg_first) {
+                    // both CTAs' drains of this buffer's previous segment are done
+                    if (!tc::wait_timed_cluster(&tempty[b], ((uint32_t)(seg >> 1) & 1u) ^ 1u, kWaitNs, &abort_flag)) {
+                        if (!abort_flag) report_fault(p.fault, kFaultTcMmaWait);
+                        abort_flag = 1;
+                        stop = true;
+                        break;
+                    }
+                    tc::fence_after_sync();
+                }
+                const int s = kb % S;
+                if (!tc::wait_timed_cluster(&full[s], (uint32_t)(kb / S) & 1u, kWaitNs, &abort_flag)) {
+                    if (!abort_flag) report_fault(p.fault, kFaultTcMmaWait);
+                    abort_flag = 1;
+                    stop = true;
+                    break;
+                }
+                tc::fence_after_sync();
+                const uint32_t d = tmem + (uint32_t)(b * 256);
+#pragma unroll
+                for (int kk = 0; kk < L::KSTEPS; ++kk) {
+#pragma unroll
+                    for (int j = 0; j < MD::NPROD; ++j) {
+                        const uint32_t a_addr = smem_u32(a_tile(s, MD::pa(j))) + kk * 32;
+                        const uint32_t b_addr = smem_u32(b_tile(s, MD::pb(j))) + kk * 32;
+                        const uint64_t ad = tc::smem_desc_kmajor(a_addr, L::SBO, L::SWIZZLE);
+                        const uint64_t bd = tc::smem_desc_kmajor(b_addr, L::SBO, L::SWIZZLE);
+                        const uint32_t accum = (seg_first && kk == 0 && j == 0) ? 0u : 1u;
+                        if constexpr (MD::SCALED) tc::mma_f8_pair(d, ad, bd, idesc, accum);
+                        else tc::mma_bf16_pair(d, ad, bd, idesc, accum);
+                    }
+                }
+                const uint32_t so = (uint32_t)(s * sizeof(uint64_t)), bo = (uint32_t)(b * sizeof(uint64_t));
+                tc::commit_pair_to(empty_self + so);
+                tc::commit_pair_to(empty_peer + so);
+                if (seg_last) {
+                    tc::commit_pair_to(tfull_self + bo);
+                    tc::commit_pair_to(tfull_peer + bo);
+                }
+            }
+            kb_consumed = kb;
+            if (stop) {
+                mma_aborted = 1;
+                tc::commit_pair_to(tc::mapa_shared(smem_u32(&mma_done), 0));
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---- drain (both CTAs): promote each segment into FP32 registers ----
+        const int quarter = warp & 3, half = (warp - 2) >> 2;
+        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+        float acc[128];
+#pragma unroll
+        for (int j = 0; j < 128; ++j) acc[j] = 0.0f;
+        bool ok = true;
+        for (int seg = 0; seg < nseg; ++seg) {
+            const int b = seg & 1;
+            float scale = 1.0f;
+            if constexpr (MD::SCALED) scale = half ? seg_q1[seg] : seg_q0[seg];
+            if (!tc::wait_timed_cluster(&tfull[b], (uint32_t)(seg >> 1) & 1u, 2 * kWaitNs, &abort_flag)) {
+                if (!abort_flag) report_fault(p.fault, kFaultTcEpilogueWait);
+                abort_flag = 1;
+                ok = false;
+                break;
+            }
+            tc::fence_after_sync();
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                uint32_t r[32];
+                tc::tmem_ld_32x32b_x32(tmem + lane_base + (uint32_t)(b * 256 + half * 128 + c * 32), r);
+                tc::tmem_ld_wait();
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    if constexpr (MD::SCALED)
+                        acc[c * 32 + j] = __fmaf_rn(__uint_as_float(r[j]), scale, acc[c * 32 + j]);
+                    else
+                        acc[c * 32 + j] = __fadd_rn(acc[c * 32 + j], __uint_as_float(r[j]));
+                }
+            }
+            tc::fence_before_sync();
+            __syncwarp();
+            if (lane == 0) {
+                if (leader) mbar_arrive(&tempty[b]);
+                else tc::mbar_arrive_remote(tempty_leader + (uint32_t)(b * sizeof(uint64_t)));
+            }
+        }
+        if (ok && !abort_flag) {
+            const int64_t row = (int64_t)m0 + quarter * 32 + lane;
+            float *crow = p.C + (int64_t)z * p.stride_c + row * p.ldc;
+            const bool vec_ok = (p.ldc % 4 == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0) &&
+                                (p.stride_c % 4 == 0);
+            if (row < p.M) {
+                const int64_t col0 = (int64_t)n0 + half * 128;
+#pragma unroll
+                for (int j = 0; j < 128; j += 4) {
+                    float v[4];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const int64_t col = col0 + j + e;
+                        if (p.gemm) {
+                            const float bc = (p.beta == 0.0f || col >= p.N) ? 0.0f : p.beta * crow[col];
+                            v[e] = __fmaf_rn(p.alpha, acc[j + e], bc);
+                        } else {
+                            v[e] = acc[j + e];
+                        }
+                    }
+                    if (vec_ok && col0 + j + 3 < p.N) {
+                        *reinterpret_cast<float4 *>(crow + col0 + j) = make_float4(v[0], v[1], v[2], v[3]);
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < 4; ++e)
+                            if (col0 + j + e < p.N) crow[col0 + j + e] = v[e];
+                    }
+                }
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (threadIdx.x == 0 && abort_flag) {
+        // This CTA's copies complete on the leader's barrier, so they cannot be
+        // awaited here: give them time to land (they take microseconds).  The
+        // leader also waits for the MMAs issued before its abort.
+        const uint64_t t0 = tc::globaltimer();
+        while (tc::globaltimer() - t0 < 20000000ull) {
+        }
+        if (leader && mma_aborted) tc::wait_timed(&mma_done, 0, kWaitNs, nullptr);
+    }
+    __syncthreads();
+    tc::cluster_sync();  // neither CTA leaves while the pair can still touch its memory
+    if (warp == 0) tc::tmem_dealloc_pair(tmem, kTmemCols2);
 }
 
 // ---------------------------------------------------------------------------
@@ -592,17 +957,24 @@ static WsPtrs ws_ptrs(const Plan &pl, void *ws) {
     return w;
 }
 
+// CTA pairs (256 x 256 tiles) for M > 128: 1 = where they measure faster on
+// B200 (the six-product engine: 264 vs 239 TFLOP/s at 8192^3; BF16, split3
+// and FP8 run faster as single CTAs), 2 = always, 0 = never.
+static int g_tc_pair = 1;
+
 template <int MODE>
 static int launch_tc(const Geometry &g, const Plan &pl, const WsPtrs &w, float *C, double alpha, double beta,
                      int gemm, int seg_kblocks, cudaStream_t stream) {
     using L = Layout<MODE>;
+    const bool pair = g.M > BM && (g_tc_pair == 2 || (g_tc_pair == 1 && MODE == 2));
     CUtensorMap ta[3], tb[3];
     const uint64_t row_bytes = (uint64_t)pl.Kp * pl.elem;
     const uint64_t adims[3] = {(uint64_t)pl.Kp, (uint64_t)g.M, (uint64_t)g.batch};
     const uint64_t astr[2] = {row_bytes, row_bytes * (uint64_t)g.M};
     const uint64_t bdims[3] = {(uint64_t)pl.Kp, (uint64_t)g.N, (uint64_t)g.batch};
     const uint64_t bstr[2] = {row_bytes, row_bytes * (uint64_t)g.N};
-    const uint32_t abox[3] = {(uint32_t)L::BK, BM, 1}, bbox[3] = {(uint32_t)L::BK, BN, 1};
+    // a CTA of a pair stages 128 rows of B (its half of the pair's 256 columns)
+    const uint32_t abox[3] = {(uint32_t)L::BK, BM, 1}, bbox[3] = {(uint32_t)L::BK, pair ? 128u : (uint32_t)BN, 1};
     const CUtensorMapDataType dt = MODE == 3 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
     const CUtensorMapSwizzle swz = L::ROW_BYTES == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
     for (int i = 0; i < 3; ++i) {
@@ -619,7 +991,7 @@ static int launch_tc(const Geometry &g, const Plan &pl, const WsPtrs &w, float *
     p.ldc = g.ldc;
     p.stride_c = g.stride_c;
     p.kblocks = (int)((pl.Kp + L::BK - 1) / L::BK);
-    p.seg_kblocks = Mode<MODE>::SCALED ? 1 : (seg_kblocks > 0 ? seg_kblocks : kDefaultSegKblocks);
+    p.seg_kblocks = seg_kblocks > 0 ? seg_kblocks : kDefaultSegKblocks;
     p.alpha = (float)alpha;
     p.beta = (float)beta;
     p.gemm = gemm;
@@ -629,7 +1001,34 @@ static int launch_tc(const Geometry &g, const Plan &pl, const WsPtrs &w, float *
     p.scale_a_stride = pl.mblocks * pl.kblocks;
     p.scale_b_stride = pl.nblocks * pl.kblocks;
     p.nblocks_n = (int)pl.nblocks;
+    p.nblocks_m = (int)pl.mblocks;
     if (MODE == 3 && p.kblocks != pl.kblocks) return set_error(GATLAS_ERR_INVALID, "matmul: FP8 slice count");
+    if (MODE == 3 && p.kblocks > kMaxFp8Blocks)
+        return set_error(GATLAS_ERR_UNSUPPORTED, "matmul: FP8 engine takes K <= %d", kMaxFp8Blocks * 128);
+    if (pair) {
+        using PL = PairLayout<MODE>;
+        const int smem = (int)PL::SMEM_BYTES;
+        cudaError_t e =
+            cudaFuncSetAttribute(tc_gemm_pair_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "tc pair smem attribute: %s", cudaGetErrorString(e));
+        const int64_t pairs = ((g.M + PL::PM - 1) / PL::PM) * ((g.N + PL::PN - 1) / PL::PN);
+        if (2 * pairs > 0x7fffffff) return set_error(GATLAS_ERR_INVALID, "matmul: too many tensor-core tiles");
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(2 * pairs), 1, (unsigned)g.batch);
+        cfg.blockDim = dim3(kThreads2, 1, 1);
+        cfg.dynamicSmemBytes = (size_t)smem;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        e = cudaLaunchKernelEx(&cfg, tc_gemm_pair_kernel<MODE>, ta[0], ta[1], ta[2], tb[0], tb[1], tb[2], p);
+        if (e != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "tc_gemm_pair_kernel: %s", cudaGetErrorString(e));
+        return check_launch("tc_gemm_pair_kernel");
+    }
     const int smem = (int)L::SMEM_BYTES;
     cudaError_t e = cudaFuncSetAttribute(tc_gemm_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "tc gemm smem attribute: %s", cudaGetErrorString(e));
@@ -725,6 +1124,27 @@ int matmul_tc(const gatlas_matmul_desc *d, const Geometry &g, const float *A, co
 }
 
 }  // namespace gatlas
+
+extern "C" int gatlas_set_option(const char *name, int64_t value) {
+    using namespace gatlas;
+    if (!name) return set_error(GATLAS_ERR_INVALID, "set_option: null name");
+    if (std::strcmp(name, "tc_pair") == 0) {
+        if (value < 0 || value > 2) return set_error(GATLAS_ERR_INVALID, "set_option: tc_pair is 0, 1 or 2");
+        tcg::g_tc_pair = (int)value;
+        return GATLAS_OK;
+    }
+    return set_error(GATLAS_ERR_INVALID, "set_option: unknown option %s", name);
+}
+
+extern "C" int gatlas_get_option(const char *name, int64_t *value) {
+    using namespace gatlas;
+    if (!name || !value) return set_error(GATLAS_ERR_INVALID, "get_option: null argument");
+    if (std::strcmp(name, "tc_pair") == 0) {
+        *value = tcg::g_tc_pair;
+        return GATLAS_OK;
+    }
+    return set_error(GATLAS_ERR_INVALID, "get_option: unknown option %s", name);
+}
 
 extern "C" int gatlas_matmul_tc_prepare(const gatlas_matmul_desc *d, const float *A, const float *B, void *workspace,
                                         size_t workspace_bytes, void *stream) {

@@ -16,6 +16,9 @@ constexpr int BM = 128, BN = 256;
 // K = 128 per TMEM segment (selectable per call through the descriptor's
 // extra field).  The FP8 mode promotes every slice (one scale block).
 constexpr int kDefaultSegKblocks = 4;
+// FP8: most 128-deep blocks per tile (K <= 131072), and by default at most
+// 4 equally scaled blocks accumulate in TMEM before promotion.
+constexpr int kMaxFp8Blocks = 1024;
 
 // MODE 0: one BF16 piece, one product; 1: two pieces, three products;
 // 2: three pieces, six products; 3: FP8 E4M3 codes with one FP32 scale per
@@ -67,8 +70,36 @@ struct Layout {
     static constexpr uint32_t B_TILE = BN * ROW_BYTES;
     static constexpr int KSTEPS = ROW_BYTES / 32;                   // MMA instructions per slice
     static constexpr uint32_t STAGE_BYTES = NP * (A_TILE + B_TILE);
-    static constexpr uint32_t SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + alignment slack
+    // FP8: per-block scale products of the tile's two column halves, compacted
+    // in place into per-segment scales, and one segment-start flag per block
+    static constexpr uint32_t PLAN_BYTES = MD::SCALED ? (2 * 4 + 1) * 1024 : 0;
+    static constexpr uint32_t SMEM_BYTES = STAGES * STAGE_BYTES + PLAN_BYTES + 1024;  // + alignment slack
     static constexpr uint32_t IDESC = MD::SCALED ? tc::idesc_e4m3_f32(BM, BN) : tc::idesc_bf16_f32(BM, BN);
+};
+
+// CTA-pair layout (cta_group::2): one 256 x 256 tile per pair of CTAs.  Each
+// CTA stages its 128 rows of A and its 128-row half of B per K slice, and
+// holds its 128 rows of the accumulator in its own TMEM.
+template <int MODE>
+struct PairLayout {
+    using L1 = Layout<MODE>;
+    using MD = Mode<MODE>;
+    static constexpr int NP = MD::NP;
+    static constexpr int BK = L1::BK;
+    static constexpr uint32_t ROW_BYTES = L1::ROW_BYTES;
+    static constexpr uint32_t SWIZZLE = L1::SWIZZLE;
+    static constexpr uint32_t SBO = L1::SBO;
+    static constexpr int KSTEPS = L1::KSTEPS;
+    static constexpr int PM = 256, PN = 256;                 // pair tile
+    static constexpr uint32_t A_TILE = 128 * ROW_BYTES;      // this CTA's rows of A
+    static constexpr uint32_t B_TILE = 128 * ROW_BYTES;      // this CTA's half of B
+    static constexpr uint32_t STAGE_BYTES = NP * (A_TILE + B_TILE);
+    static constexpr uint32_t PLAN_BYTES = L1::PLAN_BYTES;
+    static constexpr uint32_t BUDGET = 226 * 1024;          // dynamic shared memory per CTA
+    static constexpr int STAGES = (int)((BUDGET - PLAN_BYTES - 1024) / STAGE_BYTES);
+    static constexpr uint32_t SMEM_BYTES = STAGES * STAGE_BYTES + PLAN_BYTES + 1024;
+    static constexpr uint32_t IDESC = MD::SCALED ? tc::idesc_e4m3_f32(PM, PN) : tc::idesc_bf16_f32(PM, PN);
+    static_assert(STAGES >= 3, "pair pipeline depth");
 };
 
 template <int NP>

@@ -133,7 +133,9 @@ int gatlas_matvec_f32_noalloc(const gatlas_matvec_desc *d, const float *A, const
  * sum is added into round-to-nearest FP32 registers (0 selects 4, K = 128).
  * GATLAS_ENGINE_TC_FP8 quantises each operand to E4M3 with one power-of-two
  * FP32 scale per 128 x 128 block (the smallest power of two s with
- * amax / s <= 448) and promotes every 128-deep block scaled by sa * sb; its
+ * amax / s <= 448); runs of up to `extra` (0 selects 4) 128-deep blocks
+ * whose scale products sa * sb are equal accumulate in TMEM and are promoted
+ * scaled once, exactly (powers of two), K <= 131072; its
  * tc_prepare workspace holds [A codes][B codes][A scales][B scales], codes
  * K-major [batch][rows][Kp] (Kp = K rounded up to 16), scales
  * [batch][rows/128][K/128], each part 1024-byte aligned. */
@@ -167,6 +169,15 @@ int gatlas_matmul_tc_prepare(const gatlas_matmul_desc *d, const float *A, const 
                              size_t workspace_bytes, void *stream);
 int gatlas_matmul_tc_run(const gatlas_matmul_desc *d, const void *workspace, size_t workspace_bytes, float *C,
                          void *stream);
+
+/* Library options.  "tc_pair": whether tensor-core contractions with
+ * M > 128 run as CTA pairs (cta_group::2, a 256 x 256 tile per pair, each
+ * CTA staging half of B) or one CTA per 128 x 256 tile: 1 (default) where
+ * pairs measure faster (the six-product engine), 2 always, 0 never.  Results
+ * are bit-identical either way (same pieces, same MMA order, same
+ * promotion). */
+int gatlas_set_option(const char *name, int64_t value);
+int gatlas_get_option(const char *name, int64_t *value);
 
 /* 1 if a prebuilt kernel exists for (scalar 0=float/1=double, desc); 2 if
  * the SIMT point has no prebuilt instantiation but will be compiled on first

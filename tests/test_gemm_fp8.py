@@ -153,3 +153,38 @@ def test_full_size_error_on_the_device(cuda):
     fro, ref, _, _ = g.residual(A, B, C, M, N, K)
     assert fro / ref <= FP8_BUDGET
     assert g.device_faults() == 0
+
+
+@pytest.mark.parametrize("extra", [1, 2, 4])
+def test_segments_follow_changing_block_scales(cuda, extra):
+    # scale products change along K (A's column blocks and B's row blocks are
+    # scaled by different powers of two), so runs of equal scale break at the
+    # changes; every promotion interval gives the dequantised product
+    import torch
+    M, N, K = 256, 384, 1280
+    A, B = _operands(M, N, K, 1, seed=21)
+    A2 = A.reshape(M, K).copy()
+    B2 = B.reshape(K, N).copy()
+    for kb in range(K // 128):
+        A2[:, kb * 128:(kb + 1) * 128] *= np.float32(2.0 ** (kb % 3 - 1))
+        B2[kb * 128:(kb + 1) * 128, :128] *= np.float32(2.0 ** (kb // 4))
+    A2, B2 = A2.ravel(), B2.ravel()
+    ws = _prepare(cuda, A2, B2, M, N, K, 0, 0, 1)
+    qa, qb, sa, sb = _ws_views(ws, M, N, K, 1)
+    assert len(set(sa[0, 0].tolist())) == 3 and len(set(sb[0, 0].tolist())) > 1
+    C = torch.full((M * N,), float("nan"), device=cuda)
+    g.matmul_tc_run(ws, M, N, K, C, engine="tc_fp8", extra=extra)
+    torch.cuda.synchronize()
+    assert g.device_faults() == 0
+    ref = oracle.matmul_fp8_dequant(qa, sa, qb, sb, M, N, K)
+    assert oracle.normwise_error(C.cpu().numpy(), ref) <= PIPE_TOL
+
+
+def test_k_limit_of_the_fp8_engine(cuda):
+    import torch
+    M = N = 16
+    K = 1024 * 128 + 16
+    A = torch.zeros(M * K, device=cuda)
+    B = torch.zeros(K * N, device=cuda)
+    with pytest.raises(g.GatlasError, match="K <="):
+        g.matmul(A, B, M, N, K, engine="tc_fp8")

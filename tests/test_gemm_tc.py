@@ -132,3 +132,24 @@ def test_promotion_interval_is_selectable(cuda):
         torch.cuda.synchronize()
         errs.append(oracle.normwise_error(C.cpu().numpy(), ref))
     assert errs[0] <= errs[2] and errs[1] <= errs[2]
+
+
+@pytest.mark.parametrize("engine", ENGINES + ["tc_fp8"])
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("M,N,K", [(520, 300, 384), (256, 256, 4096), (129, 1000, 40)])
+def test_cta_pairs_match_single_ctas(cuda, engine, ta, tb, M, N, K):
+    # 256 x 256 tiles on CTA pairs (cta_group::2) and 128 x 256 tiles on single
+    # CTAs run the same pieces through the same MMA order and promotion
+    A = oracle.uniform(M * K, seed=M + K + ta)
+    B = oracle.uniform(K * N, seed=N + K + tb)
+    assert g.get_option("tc_pair") == 1
+    try:
+        g.set_option("tc_pair", 0)
+        single = _mm(cuda, A, B, M, N, K, engine, ta, tb, gemm=True, Cin=oracle.uniform(M * N, seed=3),
+                     alpha=1.5, beta=0.5)
+        g.set_option("tc_pair", 2)
+        pair = _mm(cuda, A, B, M, N, K, engine, ta, tb, gemm=True, Cin=oracle.uniform(M * N, seed=3),
+                   alpha=1.5, beta=0.5)
+    finally:
+        g.set_option("tc_pair", 1)
+    assert np.array_equal(single, pair)

@@ -5,6 +5,8 @@ import glob
 import os
 import re
 
+import pytest
+
 import gatlas_b200 as g
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -66,3 +68,17 @@ def test_workspace_queries():
     assert g.matvec_workspace_size(16384, 16384, trans_a=False) == 0
     assert g.matvec_workspace_size(16384, 16384, trans_a=True) > 0
     assert g.matmul_workspace_size(1024, 1024, 1024, "buffer") == 0
+
+
+def test_options_round_trip_without_a_device():
+    import gatlas_b200 as g
+    assert g.get_option("tc_pair") == 1
+    g.set_option("tc_pair", 0)
+    try:
+        assert g.get_option("tc_pair") == 0
+    finally:
+        g.set_option("tc_pair", 1)
+    with pytest.raises(g.GatlasError, match="unknown option"):
+        g.set_option("no_such_option", 1)
+    with pytest.raises(g.GatlasError, match="0, 1 or 2"):
+        g.set_option("tc_pair", 3)
