@@ -113,6 +113,7 @@ def lib() -> ctypes.CDLL:
     L.gatlas_matmul_residual_f32.argtypes = [ctypes.POINTER(MatmulDesc), vp, vp, vp,
                                              ctypes.POINTER(ctypes.c_double), vp]
     L.gatlas_device_faults.argtypes = [ctypes.POINTER(ctypes.c_int), i32]
+    L.gatlas_matmul_f32_host.argtypes = [ctypes.POINTER(MatmulDesc), vp, vp, vp, vp]
     L.gatlas_set_option.argtypes = [ctypes.c_char_p, ctypes.c_int64]
     L.gatlas_get_option.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
     gi = ctypes.POINTER(GroupedInstance)
@@ -502,3 +503,16 @@ def get_option(name: str) -> int:
     v = ctypes.c_int64()
     check(lib().gatlas_get_option(name.encode(), ctypes.byref(v)))
     return int(v.value)
+
+
+def matmul_host(A, B, M, N, K, C, trans_a=False, trans_b=False, gemm=False, alpha=1.0, beta=0.0,
+                engine="tc_split3", batch=1, extra=0, stream=None):
+    """C = op(A)op(B) with host (CPU, ideally pinned) float32 tensors: upload,
+    contract and download in one call, ordered on the current CUDA stream."""
+    for t in (A, B, C):
+        if t is not None and t.is_cuda:
+            raise ValueError("matmul_host takes host tensors")
+    d = matmul_desc(M, N, K, trans_a, trans_b, gemm, alpha, beta, engine, batch=batch,
+                    tile=(0, 0, 0, 0, 0, extra))
+    check(lib().gatlas_matmul_f32_host(ctypes.byref(d), _ptr(A), _ptr(B), _ptr(C), _stream(stream)))
+    return C

@@ -10,8 +10,9 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 int *g_fault[kMaxDevices] = {nullptr};
-void *g_scratch[kMaxDevices] = {nullptr};
-size_t g_scratch_bytes[kMaxDevices] = {0};
+void *g_scratch[kScratchSlots][kMaxDevices] = {{nullptr}};
+size_t g_scratch_bytes[kScratchSlots][kMaxDevices] = {{0}};
+cudaStream_t g_streams[kMaxDevices][kPoolStreams] = {{nullptr}};
 
 int current_device() {
     int dev = -1;
@@ -36,25 +37,39 @@ int *device_fault_word() {
     return g_fault[dev];
 }
 
-void *device_scratch(size_t bytes) {
+void *device_scratch(size_t bytes, int slot) {
     const int dev = current_device();
-    if (dev < 0) return nullptr;
+    if (dev < 0 || slot < 0 || slot >= kScratchSlots) return nullptr;
     std::lock_guard<std::mutex> lk(g_mu);
-    if (g_scratch_bytes[dev] < bytes) {
-        if (g_scratch[dev]) {
+    if (g_scratch_bytes[slot][dev] < bytes) {
+        if (g_scratch[slot][dev]) {
             cudaDeviceSynchronize();
-            cudaFree(g_scratch[dev]);
-            g_scratch[dev] = nullptr;
-            g_scratch_bytes[dev] = 0;
+            cudaFree(g_scratch[slot][dev]);
+            g_scratch[slot][dev] = nullptr;
+            g_scratch_bytes[slot][dev] = 0;
         }
         // round up to 2 MiB so that slowly growing requests do not reallocate often
         const size_t want = (bytes + ((size_t)2 << 20) - 1) & ~(((size_t)2 << 20) - 1);
         void *p = nullptr;
-        if (cudaMalloc(&p, want) != cudaSuccess) return nullptr;
-        g_scratch[dev] = p;
-        g_scratch_bytes[dev] = want;
+        if (cudaMalloc(&p, want) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        g_scratch[slot][dev] = p;
+        g_scratch_bytes[slot][dev] = want;
     }
-    return g_scratch[dev];
+    return g_scratch[slot][dev];
+}
+
+cudaStream_t pool_stream(int i) {
+    const int dev = current_device();
+    if (dev < 0 || i < 0 || i >= kPoolStreams) return nullptr;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_streams[dev][i] && cudaStreamCreateWithFlags(&g_streams[dev][i], cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        g_streams[dev][i] = nullptr;
+    }
+    return g_streams[dev][i];
 }
 
 }  // namespace gatlas

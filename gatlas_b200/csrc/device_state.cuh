@@ -21,9 +21,16 @@ enum FaultCode : int {
 // first use); nullptr if the allocation failed.
 int *device_fault_word();
 
-// Current device's cached scratch buffer of at least `bytes` (grown on demand,
-// never shrunk).  nullptr on failure.  Not safe to grow during graph capture.
-void *device_scratch(size_t bytes);
+// Current device's cached scratch buffer `slot` of at least `bytes` (grown on
+// demand, never shrunk).  Slot 0 serves the engines' workspaces, slot 1 the
+// device copies of the host-buffer entry points.  nullptr on failure.  Not
+// safe to grow during graph capture.
+constexpr int kScratchSlots = 2;
+void *device_scratch(size_t bytes, int slot = 0);
+
+// Per-device non-blocking streams owned by the library (created on first use).
+constexpr int kPoolStreams = 2;
+cudaStream_t pool_stream(int i);
 
 #ifdef __CUDACC__
 __device__ __forceinline__ void report_fault(int *word, int code) {

@@ -344,7 +344,7 @@ std::ostream &KernelMatmul::print(std::ostream &os) const {
         os << "// tcgen05 kernel tc_gemm_kernel<" << variant_name(variant_)
            << ">: 128x256 output tile per CTA, TMA 64B-swizzled BF16 piece tiles (BK=32), "
            << "tcgen05.mma kind::f16 M=128 N=256 K=16, FP32 accumulation in TMEM promoted every "
-           << (extraParam() ? extraParam() : 4) << " K-slices\n";
+           << (extraParam() ? extraParam() : (variant_ == Variant::TcBf16 ? 16 : 4)) << " K-slices\n";
     } else {
         const size_t bm = groupHeight() * blockHeight(), bn = groupWidth() * blockWidth();
         const bool img = variant_ == Variant::Image;

@@ -247,6 +247,47 @@ extern "C" int gatlas_matmul_f32(const gatlas_matmul_desc *d, const float *A, co
     return gatlas::matmul_dispatch<float>(d, A, B, C, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
+// Host buffers in, host buffer out (the reference's bus-transfer timing
+// modes, GatlasBenchmark.cpp:198-265, as one call).  Tensor-core engines with
+// M >= 2048 and one instance run as a pipeline: B is uploaded and prepared
+// once, then A streams in blocks of 1024 rows whose uploads, preparation,
+// contraction and C downloads overlap on two library streams.  Everything
+// else uploads the operands, runs the engine and downloads C on `stream`.
+extern "C" int gatlas_matmul_f32_host(const gatlas_matmul_desc *d, const float *A, const float *B, float *C,
+                                      void *stream) {
+    using namespace gatlas;
+    if (!d) return set_error(GATLAS_ERR_INVALID, "matmul_host: null descriptor");
+    Geometry g;
+    if (!resolve_geometry(d, &g)) return set_error(GATLAS_ERR_INVALID, "matmul_host: invalid dimensions");
+    if (g.M == 0 || g.N == 0) return GATLAS_OK;
+    if (!C || (g.K > 0 && (!A || !B))) return set_error(GATLAS_ERR_INVALID, "matmul_host: null pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    const bool tc = d->engine >= GATLAS_ENGINE_TC_BF16 && d->engine <= GATLAS_ENGINE_TC_FP8;
+    if (tc && tcg::host_pipeline_ok(d, g)) {
+        void *dev = device_scratch(tcg::host_pipeline_bytes(d, g), 1);
+        if (!dev) return set_error(GATLAS_ERR_NOMEM, "matmul_host: device copies");
+        return tcg::host_pipeline(d, g, A, B, C, dev, s);
+    }
+    const int64_t a_rows = g.ta ? g.K : g.M, b_rows = g.tb ? g.N : g.K;
+    const size_t a_el = g.K ? (size_t)((g.batch - 1) * g.stride_a + a_rows * g.lda) : 0;
+    const size_t b_el = g.K ? (size_t)((g.batch - 1) * g.stride_b + b_rows * g.ldb) : 0;
+    const size_t c_el = (size_t)((g.batch - 1) * g.stride_c + g.M * g.ldc);
+    auto r1k = [](size_t b) { return (b + 1023) / 1024 * 1024; };
+    uint8_t *dev = static_cast<uint8_t *>(device_scratch(r1k(a_el * 4) + r1k(b_el * 4) + r1k(c_el * 4) + 1024, 1));
+    if (!dev) return set_error(GATLAS_ERR_NOMEM, "matmul_host: device copies");
+    float *dA = reinterpret_cast<float *>(dev), *dB = reinterpret_cast<float *>(dev + r1k(a_el * 4));
+    float *dC = reinterpret_cast<float *>(dev + r1k(a_el * 4) + r1k(b_el * 4));
+    if ((a_el && cudaMemcpyAsync(dA, A, a_el * 4, cudaMemcpyHostToDevice, s) != cudaSuccess) ||
+        (b_el && cudaMemcpyAsync(dB, B, b_el * 4, cudaMemcpyHostToDevice, s) != cudaSuccess) ||
+        (d->gemm && d->beta != 0.0 && cudaMemcpyAsync(dC, C, c_el * 4, cudaMemcpyHostToDevice, s) != cudaSuccess))
+        return check_launch("matmul_host upload");
+    const int rc = gatlas_matmul_f32(d, dA, dB, dC, nullptr, 0, stream);
+    if (rc) return rc;
+    if (cudaMemcpyAsync(C, dC, c_el * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return check_launch("matmul_host download");
+    return GATLAS_OK;
+}
+
 extern "C" int gatlas_matmul_f64(const gatlas_matmul_desc *d, const double *A, const double *B, double *C,
                                  void *workspace, size_t workspace_bytes, void *stream) {
     return gatlas::matmul_dispatch<double>(d, A, B, C, workspace, workspace_bytes, (cudaStream_t)stream);

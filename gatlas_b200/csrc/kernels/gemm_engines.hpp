@@ -51,5 +51,12 @@ int matmul_tc(const gatlas_matmul_desc *d, const Geometry &g, const float *A, co
               void *ws, size_t ws_bytes, cudaStream_t stream);
 int tc_supported(const gatlas_matmul_desc *d);
 size_t tc_workspace_bytes(const gatlas_matmul_desc *d, const Geometry &g);
+namespace tcg {
+// host-buffer pipeline of the tensor-core engines (gemm_tc.cu)
+bool host_pipeline_ok(const gatlas_matmul_desc *d, const Geometry &g);
+size_t host_pipeline_bytes(const gatlas_matmul_desc *d, const Geometry &g);
+int host_pipeline(const gatlas_matmul_desc *d, const Geometry &g, const float *hA, const float *hB, float *hC,
+                  void *dev, cudaStream_t caller);
+}  // namespace tcg
 
 }  // namespace gatlas

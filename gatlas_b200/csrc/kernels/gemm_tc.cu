@@ -24,6 +24,7 @@
 // fault word, stops the pipeline, drains the copies in flight and frees TMEM.
 #include <cuda.h>
 
+#include <algorithm>
 #include <cstring>
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
@@ -991,7 +992,7 @@ static int launch_tc(const Geometry &g, const Plan &pl, const WsPtrs &w, float *
     p.ldc = g.ldc;
     p.stride_c = g.stride_c;
     p.kblocks = (int)((pl.Kp + L::BK - 1) / L::BK);
-    p.seg_kblocks = seg_kblocks > 0 ? seg_kblocks : kDefaultSegKblocks;
+    p.seg_kblocks = seg_kblocks > 0 ? seg_kblocks : default_seg_kblocks(MODE);
     p.alpha = (float)alpha;
     p.beta = (float)beta;
     p.gemm = gemm;
@@ -1085,6 +1086,129 @@ int tc_run(const gatlas_matmul_desc *d, const Geometry &g, const void *ws, size_
         case 2: return launch_tc<2>(g, pl, w, C, d->alpha, d->beta, d->gemm, (int)d->extra, stream);
         default: return launch_tc<3>(g, pl, w, C, d->alpha, d->beta, d->gemm, (int)d->extra, stream);
     }
+}
+
+// ---------------------------------------------------------------------------
+// host-buffer contraction: uploads, preparation, contraction and downloads of
+// row blocks of A overlap on two streams
+// ---------------------------------------------------------------------------
+constexpr int64_t kHostBlockRows = 1024;  // multiple of 256 (CTA pairs) and 128 (FP8 scale blocks)
+
+// Prepares rows [r0, r1) of A (K-major pieces or codes and scales).
+static int prepare_a_rows(const Plan &pl, const Geometry &g, const float *A, int64_t r0, int64_t r1,
+                          const WsPtrs &w, cudaStream_t s) {
+    const float *src = g.ta ? A + r0 : A + r0 * g.lda;  // stored K x M: a column block
+    const int64_t rows = r1 - r0;
+    if (pl.mode == 3)
+        return launch_quant(g.ta, src, rows, g.K, pl.Kp, g.lda, 0, 1, static_cast<uint8_t *>(w.a[0]) + r0 * pl.Kp,
+                            w.sa + (r0 / kQBlock) * pl.kblocks, s);
+    __nv_bfloat16 *ap[3];
+    for (int i = 0; i < 3; ++i)
+        ap[i] = w.a[i] ? static_cast<__nv_bfloat16 *>(w.a[i]) + r0 * pl.Kp : nullptr;
+    return launch_split(pl.np, g.ta, src, rows, g.K, pl.Kp, g.lda, 0, 1, ap, s);
+}
+
+static int prepare_b(const Plan &pl, const Geometry &g, const float *B, const WsPtrs &w, cudaStream_t s) {
+    if (pl.mode == 3)
+        return launch_quant(!g.tb, B, g.N, g.K, pl.Kp, g.ldb, 0, 1, static_cast<uint8_t *>(w.b[0]), w.sb, s);
+    __nv_bfloat16 *bp[3];
+    for (int i = 0; i < 3; ++i) bp[i] = static_cast<__nv_bfloat16 *>(w.b[i]);
+    return launch_split(pl.np, !g.tb, B, g.N, g.K, pl.Kp, g.ldb, 0, 1, bp, s);
+}
+
+// Contracts rows [r0, r1) of A against all of B into rows [r0, r1) of C.
+static int run_rows(const gatlas_matmul_desc *d, const Plan &pl, const Geometry &g, const WsPtrs &w, int64_t r0,
+                    int64_t r1, float *C, cudaStream_t s) {
+    Geometry gb = g;
+    gb.M = r1 - r0;
+    Plan pb = pl;
+    pb.mblocks = (gb.M + kQBlock - 1) / kQBlock;
+    WsPtrs wb = w;
+    for (int i = 0; i < 3; ++i)
+        if (wb.a[i]) wb.a[i] = static_cast<uint8_t *>(wb.a[i]) + r0 * pl.Kp * pl.elem;
+    if (wb.sa) wb.sa += (r0 / kQBlock) * pl.kblocks;
+    float *Cb = C + r0 * g.ldc;
+    switch (pl.mode) {
+        case 0: return launch_tc<0>(gb, pb, wb, Cb, d->alpha, d->beta, d->gemm, (int)d->extra, s);
+        case 1: return launch_tc<1>(gb, pb, wb, Cb, d->alpha, d->beta, d->gemm, (int)d->extra, s);
+        case 2: return launch_tc<2>(gb, pb, wb, Cb, d->alpha, d->beta, d->gemm, (int)d->extra, s);
+        default: return launch_tc<3>(gb, pb, wb, Cb, d->alpha, d->beta, d->gemm, (int)d->extra, s);
+    }
+}
+
+// Bytes of device memory the pipeline needs: copies of A, B, C and the workspace.
+size_t host_pipeline_bytes(const gatlas_matmul_desc *d, const Geometry &g) {
+    Plan pl;
+    if (!make_plan(d, g, &pl)) return 0;
+    const int64_t a_rows = g.ta ? g.K : g.M, b_rows = g.tb ? g.N : g.K;
+    return round_up((size_t)(a_rows * g.lda) * 4, 1024) + round_up((size_t)(b_rows * g.ldb) * 4, 1024) +
+           round_up((size_t)(g.M * g.ldc) * 4, 1024) + pl.total;
+}
+
+bool host_pipeline_ok(const gatlas_matmul_desc *d, const Geometry &g) {
+    Plan pl;
+    return make_plan(d, g, &pl) && g.batch == 1 && g.K > 0 && g.M >= 2 * kHostBlockRows &&
+           (pl.mode != 3 || (g.K + kQBlock - 1) / kQBlock <= kMaxFp8Blocks);
+}
+
+int host_pipeline(const gatlas_matmul_desc *d, const Geometry &g, const float *hA, const float *hB, float *hC,
+                  void *dev, cudaStream_t caller) {
+    Plan pl;
+    if (!make_plan(d, g, &pl)) return set_error(GATLAS_ERR_UNSUPPORTED, "matmul: tensor-core engine %d not built", d->engine);
+    const int64_t a_rows = g.ta ? g.K : g.M, b_rows = g.tb ? g.N : g.K;
+    uint8_t *base = static_cast<uint8_t *>(dev);
+    float *dA = reinterpret_cast<float *>(base);
+    float *dB = reinterpret_cast<float *>(base + round_up((size_t)(a_rows * g.lda) * 4, 1024));
+    float *dC = reinterpret_cast<float *>(reinterpret_cast<uint8_t *>(dB) + round_up((size_t)(b_rows * g.ldb) * 4, 1024));
+    void *ws = reinterpret_cast<uint8_t *>(dC) + round_up((size_t)(g.M * g.ldc) * 4, 1024);
+    const WsPtrs w = ws_ptrs(pl, ws);
+    cudaStream_t st[2] = {pool_stream(0), pool_stream(1)};
+    if (!st[0] || !st[1]) return set_error(GATLAS_ERR_CUDA, "matmul: library streams");
+    cudaEvent_t ev_start, ev_b, ev_done[2];
+    if (cudaEventCreateWithFlags(&ev_start, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_b, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_done[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_done[1], cudaEventDisableTiming) != cudaSuccess)
+        return set_error(GATLAS_ERR_CUDA, "matmul: events");
+    int rc = GATLAS_OK;
+    auto cuda = [&](cudaError_t e, const char *what) {
+        if (e != cudaSuccess && rc == GATLAS_OK) rc = set_error(GATLAS_ERR_CUDA, "matmul host path: %s: %s", what, cudaGetErrorString(e));
+    };
+    cuda(cudaEventRecord(ev_start, caller), "record");
+    cuda(cudaStreamWaitEvent(st[0], ev_start, 0), "wait");
+    cuda(cudaStreamWaitEvent(st[1], ev_start, 0), "wait");
+    // B first: uploaded and prepared once on stream 0
+    cuda(cudaMemcpyAsync(dB, hB, (size_t)(b_rows * g.ldb) * 4, cudaMemcpyHostToDevice, st[0]), "upload B");
+    if (!rc) rc = prepare_b(pl, g, dB, w, st[0]);
+    cuda(cudaEventRecord(ev_b, st[0]), "record");
+    const bool read_c = d->gemm && d->beta != 0.0;
+    for (int64_t r0 = 0, blk = 0; r0 < g.M && !rc; r0 += kHostBlockRows, ++blk) {
+        const int64_t r1 = std::min(g.M, r0 + kHostBlockRows), rows = r1 - r0;
+        cudaStream_t s = st[blk & 1];
+        if (g.ta)  // stored K x M: rows r0..r1 of op(A) are a column block of every stored row
+            cuda(cudaMemcpy2DAsync(dA + r0, g.lda * 4, hA + r0, g.lda * 4, rows * 4, g.K, cudaMemcpyHostToDevice, s),
+                 "upload A");
+        else
+            cuda(cudaMemcpyAsync(dA + r0 * g.lda, hA + r0 * g.lda, (size_t)(rows * g.lda) * 4, cudaMemcpyHostToDevice,
+                                 s),
+                 "upload A");
+        if (read_c)
+            cuda(cudaMemcpy2DAsync(dC + r0 * g.ldc, g.ldc * 4, hC + r0 * g.ldc, g.ldc * 4, g.N * 4, rows,
+                                   cudaMemcpyHostToDevice, s),
+                 "upload C");
+        if (!rc) rc = prepare_a_rows(pl, g, dA, r0, r1, w, s);
+        cuda(cudaStreamWaitEvent(s, ev_b, 0), "wait");  // only the contraction needs B
+        if (!rc) rc = run_rows(d, pl, g, w, r0, r1, dC, s);
+        cuda(cudaMemcpy2DAsync(hC + r0 * g.ldc, g.ldc * 4, dC + r0 * g.ldc, g.ldc * 4, g.N * 4, rows,
+                               cudaMemcpyDeviceToHost, s),
+             "download C");
+    }
+    cuda(cudaEventRecord(ev_done[0], st[0]), "record");
+    cuda(cudaEventRecord(ev_done[1], st[1]), "record");
+    cuda(cudaStreamWaitEvent(caller, ev_done[0], 0), "wait");
+    cuda(cudaStreamWaitEvent(caller, ev_done[1], 0), "wait");
+    for (cudaEvent_t e : {ev_start, ev_b, ev_done[0], ev_done[1]}) cudaEventDestroy(e);
+    return rc;
 }
 
 }  // namespace tcg

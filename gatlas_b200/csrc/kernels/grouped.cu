@@ -609,7 +609,7 @@ static int launch_grouped(const GroupedTables &t, const GroupedDevice &d, cudaSt
     grp::Params prm;
     prm.tiles = d.tiles;
     prm.cta_start = d.cta;
-    prm.seg_kblocks = tcg::kDefaultSegKblocks;
+    prm.seg_kblocks = tcg::default_seg_kblocks(MODE);
     prm.fault = device_fault_word();
     const int smem = (int)L::SMEM_BYTES;
     static thread_local int attr_set[2] = {-1, -1};  // device whose attribute was set

@@ -16,6 +16,13 @@ constexpr int BM = 128, BN = 256;
 // K = 128 per TMEM segment (selectable per call through the descriptor's
 // extra field).  The FP8 mode promotes every slice (one scale block).
 constexpr int kDefaultSegKblocks = 4;
+// One-product BF16 promotes every 16 slices (K = 512): its MMA segment of 4
+// slices is shorter than the drain, and the longer TMEM accumulation adds
+// nothing measurable next to BF16's own input rounding (2^-9).
+constexpr int kDefaultSegKblocksBf16 = 16;
+__host__ __device__ constexpr int default_seg_kblocks(int mode) {
+    return mode == 0 ? kDefaultSegKblocksBf16 : kDefaultSegKblocks;
+}
 // FP8: most 128-deep blocks per tile (K <= 131072), and by default at most
 // 4 equally scaled blocks accumulate in TMEM before promotion.
 constexpr int kMaxFp8Blocks = 1024;

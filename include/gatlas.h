@@ -130,7 +130,8 @@ int gatlas_matvec_f32_noalloc(const gatlas_matvec_desc *d, const float *A, const
  * element, bit-exact against a sequential fmaf chain.  For the TC_* engines
  * the tile fields are ignored and `extra` is the promotion interval: the
  * tensor cores accumulate `extra` slices of K = 32 in TMEM before the partial
- * sum is added into round-to-nearest FP32 registers (0 selects 4, K = 128).
+ * sum is added into round-to-nearest FP32 registers (0 selects 4, K = 128;
+ * 16, K = 512, for the one-product BF16 engine).
  * GATLAS_ENGINE_TC_FP8 quantises each operand to E4M3 with one power-of-two
  * FP32 scale per 128 x 128 block (the smallest power of two s with
  * amax / s <= 448); runs of up to `extra` (0 selects 4) 128-deep blocks
@@ -169,6 +170,17 @@ int gatlas_matmul_tc_prepare(const gatlas_matmul_desc *d, const float *A, const 
                              size_t workspace_bytes, void *stream);
 int gatlas_matmul_tc_run(const gatlas_matmul_desc *d, const void *workspace, size_t workspace_bytes, float *C,
                          void *stream);
+
+/* Host buffers in and out: uploads op(A), op(B) (and C when gemm and
+ * beta != 0), contracts and downloads C, ordered on `stream` (the call
+ * returns before the work completes; synchronise the stream before reading
+ * C).  Replaces the reference's bus-transfer timing modes -s/-r
+ * (GatlasBenchmark.cpp:198-265).  Tensor-core engines with one instance and
+ * M >= 2048 pipeline the transfers: B is uploaded and prepared once, then A
+ * streams in blocks of 1024 rows whose uploads, preparation, contraction and
+ * C downloads overlap on two library streams.  Use pinned host memory for
+ * the copies to overlap.  Results are bit-identical to gatlas_matmul_f32. */
+int gatlas_matmul_f32_host(const gatlas_matmul_desc *d, const float *A, const float *B, float *C, void *stream);
 
 /* Library options.  "tc_pair": whether tensor-core contractions with
  * M > 128 run as CTA pairs (cta_group::2, a 256 x 256 tile per pair, each

@@ -153,3 +153,36 @@ def test_cta_pairs_match_single_ctas(cuda, engine, ta, tb, M, N, K):
     finally:
         g.set_option("tc_pair", 1)
     assert np.array_equal(single, pair)
+
+
+@pytest.mark.parametrize("engine", ENGINES + ["tc_fp8", "buffer"])
+@pytest.mark.parametrize("ta,tb", [(0, 0), (1, 1), (1, 0)])
+def test_host_buffer_entry_matches_device_path(cuda, engine, ta, tb):
+    # M = 2560: the tensor-core engines pipeline three row blocks (the last ragged);
+    # the SIMT engine takes the plain upload / run / download path
+    import torch
+    M, N, K = 2560, 384, 300
+    A = oracle.uniform(M * K, seed=5 + ta)
+    B = oracle.uniform(K * N, seed=6 + tb)
+    C0 = oracle.uniform(M * N, seed=7)
+    dev = _mm(cuda, A, B, M, N, K, engine, ta, tb, gemm=True, Cin=C0, alpha=0.5, beta=2.0)
+    hA = torch.from_numpy(A).pin_memory()
+    hB = torch.from_numpy(B).pin_memory()
+    hC = torch.from_numpy(C0.copy()).pin_memory()
+    g.matmul_host(hA, hB, M, N, K, hC, trans_a=ta, trans_b=tb, gemm=True, alpha=0.5, beta=2.0, engine=engine)
+    torch.cuda.synchronize()
+    assert g.device_faults() == 0
+    assert np.array_equal(hC.numpy(), dev)
+
+
+def test_host_buffer_entry_small_and_pageable(cuda):
+    import torch
+    M, N, K = 100, 70, 50
+    A = oracle.uniform(M * K, seed=1)
+    B = oracle.uniform(K * N, seed=2)
+    hC = torch.zeros(M * N)
+    g.matmul_host(torch.from_numpy(A), torch.from_numpy(B), M, N, K, hC, engine="tc_split3")
+    torch.cuda.synchronize()
+    assert np.array_equal(hC.numpy(), _mm(cuda, A, B, M, N, K, "tc_split3"))
+    with pytest.raises(ValueError):
+        g.matmul_host(torch.from_numpy(A).to(cuda), torch.from_numpy(B), M, N, K, hC)
