@@ -353,7 +353,7 @@ std::ostream &KernelMatmul::print(std::ostream &os) const {
            << ", GW=" << groupWidth() << ", BH=" << blockHeight() << ", BW=" << blockWidth();
         if (img)
             os << ", BK=" << (scalar_ == Scalar::Double ? 16 : 32)
-               << ">: operand tiles by TMA tensor maps through a 3-stage mbarrier ring\n";
+               << ">: operand tiles by TMA tensor maps through a 2-stage mbarrier ring\n";
         else
             os << ", VL=" << vl_ << ", BK=8>\n";
         os

@@ -73,7 +73,7 @@ int img_smem_bytes(int scalar, bool ta, bool tb, int gh, int gw, int bh, int bw)
     const int align = 1024 / es;
     const int a_raw = (BM * BK + align - 1) / align * align, b_raw = (BN * BK + align - 1) / align * align;
     const int PA = ta ? BM : BM + 4, PB = tb ? BN + 4 : BN;
-    return (3 * (a_raw + b_raw) + (ta ? 0 : BK * PA) + (tb ? BK * PB : 0)) * es + 1024;  // + alignment slack
+    return (2 * (a_raw + b_raw) + (ta ? 0 : BK * PA) + (tb ? BK * PB : 0)) * es + 1024;  // + alignment slack
 }
 
 template <typename T>

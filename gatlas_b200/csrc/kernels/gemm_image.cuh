@@ -58,7 +58,7 @@ struct ImgTile {
     static constexpr int BK = Bk<T>::value;
     static constexpr int NT = GH * GW;
     static constexpr int BM = GH * BH, BN = GW * BW;
-    static constexpr int S = 3;
+    static constexpr int S = 2;  // two stages and two CTAs per SM hide the TMA latency
     static constexpr int ALIGN = 1024 / (int)sizeof(T);                // raw tiles start on 1 KiB
     static constexpr int A_BOX = BM * BK, B_BOX = BN * BK;             // elements delivered per stage
     static constexpr int A_RAW = (A_BOX + ALIGN - 1) / ALIGN * ALIGN;  // padded slots
@@ -134,7 +134,7 @@ __device__ __forceinline__ float img_fma(float a, float b, float c) { return __f
 __device__ __forceinline__ double img_fma(double a, double b, double c) { return __fma_rn(a, b, c); }
 
 template <typename T, bool TA, bool TB, int GH, int GW, int BH, int BW>
-__global__ void __launch_bounds__(GH *GW)
+__global__ void __launch_bounds__(GH *GW, (GH * GW <= 256) ? 2 : 1)
     gemm_image_kernel(const __grid_constant__ TmapBlob mapA, const __grid_constant__ TmapBlob mapB, ImgArgs<T> a) {
     using L = ImgTile<T, TA, TB, GH, GW, BH, BW>;
     constexpr int BK = L::BK, BM = L::BM, BN = L::BN, S = L::S, NT = L::NT;

@@ -751,25 +751,28 @@ __device__ __forceinline__ uint32_t e4m3_pack4(float s, float x0, float x1, floa
     return b0 | (b1 << 8) | (b2 << 16) | (b3 << 24);
 }
 
-__global__ void __launch_bounds__(256) quant_fp8_kernel(QuantArgs a) {
+constexpr int kQThreads = 512;  // 32 values per thread; two CTAs (1024 threads) per SM
+
+__global__ void __launch_bounds__(kQThreads, 2) quant_fp8_kernel(QuantArgs a) {
+    constexpr int G = kQBlock * kQBlock / 4 / kQThreads;  // groups of 4 values per thread
     __shared__ uint32_t qt[kQBlock * 32];
-    __shared__ float red[8];
+    __shared__ float red[kQThreads / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int64_t r0 = (int64_t)blockIdx.y * kQBlock, k0 = (int64_t)blockIdx.x * kQBlock, z = blockIdx.z;
     const float *src = a.src + z * a.src_stride;
-    // 64 values per thread as 16 groups of 4 consecutive elements of the
+    // 4*G values per thread as G groups of 4 consecutive elements of the
     // stored inner dimension (k for direct sources, rows for transposed ones)
-    float v[64];
+    float v[4 * G];
     float amax = 0.0f;
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
+    for (int i = 0; i < G; ++i) {
         int64_t outer, inner;  // stored coordinates of the group's first element
         if (!a.transposed) {
-            const int idx = i * 256 + tid;                  // row idx/32, k quad idx%32
+            const int idx = i * kQThreads + tid;            // row idx/32, k quad idx%32
             outer = r0 + (idx >> 5);
             inner = k0 + (idx & 31) * 4;
         } else {
-            const int blk = (i >> 2) * 256 + tid;           // 4x4 block: row quad blk%32, k quad blk/32
+            const int blk = (i >> 2) * kQThreads + tid;     // 4x4 block: row quad blk%32, k quad blk/32
             outer = k0 + (blk >> 5) * 4 + (i & 3);
             inner = r0 + (blk & 31) * 4;
         }
@@ -778,7 +781,7 @@ __global__ void __launch_bounds__(256) quant_fp8_kernel(QuantArgs a) {
         if (outer < outer_lim) {
             const float *ptr = src + outer * a.ld + inner;
             if (a.vec && inner + 3 < inner_lim) {
-                const float4 q = __ldg(reinterpret_cast<const float4 *>(ptr));
+                const float4 q = __ldcs(reinterpret_cast<const float4 *>(ptr));
                 x[0] = q.x, x[1] = q.y, x[2] = q.z, x[3] = q.w;
             } else {
 #pragma unroll
@@ -798,7 +801,7 @@ __global__ void __launch_bounds__(256) quant_fp8_kernel(QuantArgs a) {
     __syncthreads();
     amax = red[0];
 #pragma unroll
-    for (int w = 1; w < 8; ++w) amax = fmaxf(amax, red[w]);
+    for (int w = 1; w < kQThreads / 32; ++w) amax = fmaxf(amax, red[w]);
     // s = 2^ceil(log2(amax / 448)), the smallest power of two with amax / s <= 448:
     // with amax = f * 2^e, f in [0.5, 1), that is 2^(e - 9) for f <= 0.875, else 2^(e - 8)
     float s = 0.0f;
@@ -810,14 +813,14 @@ __global__ void __launch_bounds__(256) quant_fp8_kernel(QuantArgs a) {
     if (tid == 0) a.scales[(z * a.rblocks + blockIdx.y) * a.kblocks + blockIdx.x] = s;
     if (!a.transposed) {
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            const int idx = i * 256 + tid;
+        for (int i = 0; i < G; ++i) {
+            const int idx = i * kQThreads + tid;
             qt[qt_index(idx >> 5, idx & 31)] = e4m3_pack4(s, v[i * 4], v[i * 4 + 1], v[i * 4 + 2], v[i * 4 + 3]);
         }
     } else {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int blk = j * 256 + tid;
+        for (int j = 0; j < G / 4; ++j) {
+            const int blk = j * kQThreads + tid;
             const int rq = blk & 31, kq = blk >> 5;
             // v[(j*4 + kk)*4 + e] is element (row 4*rq + e, k 4*kq + kk)
 #pragma unroll
@@ -829,8 +832,8 @@ __global__ void __launch_bounds__(256) quant_fp8_kernel(QuantArgs a) {
     __syncthreads();
     uint8_t *codes = a.codes + z * a.rows * a.Kp;
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-        const int idx = i * 256 + tid;
+    for (int i = 0; i < kQBlock * 32 / kQThreads; ++i) {
+        const int idx = i * kQThreads + tid;
         const int r = idx >> 5, w = idx & 31;
         const int64_t row = r0 + r, k = k0 + w * 4;
         if (row < a.rows && k < a.Kp)
@@ -899,7 +902,7 @@ static int launch_quant(bool transposed, const float *src, int64_t rows, int64_t
     a.kblocks = (K + kQBlock - 1) / kQBlock;
     if (a.rblocks > 65535) return set_error(GATLAS_ERR_INVALID, "matmul: too many rows for the FP8 pass");
     dim3 gr((unsigned)a.kblocks, (unsigned)a.rblocks, (unsigned)batch);
-    quant_fp8_kernel<<<gr, 256, 0, stream>>>(a);
+    quant_fp8_kernel<<<gr, kQThreads, 0, stream>>>(a);
     return check_launch("quant_fp8_kernel");
 }
 
