@@ -104,13 +104,10 @@ static int matmul_simt(const gatlas_matmul_desc *d, const Geometry &g, const T *
     int vl = (int)d->vector_length;
     const bool defaulted = (gh == 0 && gw == 0 && bh == 0 && bw == 0);
     if (defaulted) {
-        gh = gw = 16;
-        if (scalar == 0) {
-            bh = bw = 8;
-        } else {
-            bh = 8;
-            bw = 4;
-        }
+        // the fastest measured points: 16 x 16 x 8 x 8 for float, 8 x 16 x 8 x 8 for double
+        gh = scalar ? 8 : 16;
+        gw = 16;
+        bh = bw = 8;
     }
     const int vmax = scalar ? 2 : 4;
     const int fv = feasible_vl(g, A, B, sizeof(T), vl ? vl : vmax);

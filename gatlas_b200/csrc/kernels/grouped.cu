@@ -64,8 +64,70 @@ __device__ __forceinline__ int64_t packed_offset(int64_t row, int kb, int c, int
 // ordered row block major, K slice minor.  CTA b packs the contiguous items
 // [b*per_cta, (b+1)*per_cta): one binary search for its first segment, then
 // an incremental walk, and neighbouring items read neighbouring memory.
+// Where item `it` of segment `sg` reads and writes.
+struct PackItem {
+    const Inst *I;
+    int op, kb, tr;
+    int64_t r0, k0, rows, rows_alloc, ld, K;
+    const float *src;
+    bool transposed, vec;
+};
+
+__device__ __forceinline__ PackItem pack_item(const Inst *insts, const int64_t *seg_start, int sgi, int64_t it) {
+    PackItem q;
+    q.I = insts + (sgi >> 1);
+    const Inst &I = *q.I;
+    q.op = sgi & 1;
+    const int64_t local = it - seg_start[sgi];
+    q.kb = (int)(local % I.kt);
+    q.r0 = (local / I.kt) * kPackRows;
+    q.k0 = (int64_t)q.kb * kBK;
+    q.rows = q.op ? I.N : I.M;
+    q.tr = q.op ? I.bn : BM;
+    q.rows_alloc = q.op ? (int64_t)I.nt * I.bn : (int64_t)I.mt * BM;
+    q.transposed = q.op ? (I.tb == 0) : (I.ta != 0);
+    q.src = q.op ? I.src_b : I.src_a;
+    q.ld = q.op ? I.ldb : I.lda;
+    q.vec = (q.ld % 4 == 0) && ((reinterpret_cast<uintptr_t>(q.src) & 15) == 0);
+    q.K = I.K;
+    return q;
+}
+
+// The 16 values thread `tid` contributes to an item's 128 x 32 tile: four
+// groups of 4 consecutive elements of the stored inner dimension.
+__device__ __forceinline__ void pack_load(const PackItem &q, int tid, float (&x)[16]) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int e = i * 256 + tid;
+        int64_t outer, inner, outer_lim, inner_lim;
+        if (!q.transposed) {  // element (r, k) at src[r*ld + k]: 8 threads x 4 consecutive k per row
+            outer = q.r0 + (e >> 3), inner = q.k0 + (e & 7) * 4, outer_lim = q.rows, inner_lim = q.K;
+        } else {              // element (r, k) at src[k*ld + r]: 32 threads x 4 consecutive rows per k
+            outer = q.k0 + (e >> 5), inner = q.r0 + (e & 31) * 4, outer_lim = q.K, inner_lim = q.rows;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) x[i * 4 + j] = 0.0f;
+        if (outer < outer_lim) {
+            const float *ptr = q.src + outer * q.ld + inner;
+            if (q.vec && inner + 3 < inner_lim) {
+                const float4 v = __ldcs(reinterpret_cast<const float4 *>(ptr));
+                x[i * 4] = v.x, x[i * 4 + 1] = v.y, x[i * 4 + 2] = v.z, x[i * 4 + 3] = v.w;
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (inner + j < inner_lim) x[i * 4 + j] = ptr[j];
+            }
+        }
+    }
+}
+
+// Item space: segment s = 2*instance + operand covers rows/128 x kt items,
+// ordered row block major, K slice minor.  CTA b packs the contiguous items
+// [b*per_cta, (b+1)*per_cta): one binary search for its first segment, then
+// an incremental walk, and neighbouring items read neighbouring memory.  The
+// next item's loads are in flight while the current one is split and stored.
 template <int NP>
-__global__ void __launch_bounds__(256) grouped_pack_kernel(const Inst *insts, const int64_t *seg_start, int nseg,
+__global__ void __launch_bounds__(256, 4) grouped_pack_kernel(const Inst *insts, const int64_t *seg_start, int nseg,
                                                            int64_t per_cta) {
     __shared__ float tile[kPackRows][kBK + 1];
     const int tid = threadIdx.x;
@@ -83,79 +145,38 @@ __global__ void __launch_bounds__(256) grouped_pack_kernel(const Inst *insts, co
         }
         sgi = lo;
     }
-    int64_t seg_end = seg_start[sgi + 1];
+    while (it0 >= seg_start[sgi + 1]) ++sgi;
+    PackItem cur = pack_item(insts, seg_start, sgi, it0);
+    float x[16];
+    pack_load(cur, tid, x);
     for (int64_t it = it0; it < it1; ++it) {
-        while (it >= seg_end) seg_end = seg_start[++sgi + 1];
-        const Inst &I = insts[sgi >> 1];
-        const int op = sgi & 1;
-        const int64_t local = it - seg_start[sgi];
-        const int kb = (int)(local % I.kt);
-        const int64_t r0 = (local / I.kt) * kPackRows;
-        const int64_t k0 = (int64_t)kb * kBK;
-        const int64_t rows = op ? I.N : I.M;
-        const int tr = op ? I.bn : BM;
-        const int64_t rows_alloc = op ? (int64_t)I.nt * I.bn : (int64_t)I.mt * BM;
-        const bool transposed = op ? (I.tb == 0) : (I.ta != 0);
-        const float *src = op ? I.src_b : I.src_a;
-        const int64_t ld = op ? I.ldb : I.lda;
-        const bool vec = (ld % 4 == 0) && ((reinterpret_cast<uintptr_t>(src) & 15) == 0);
-        const int64_t K = I.K;
         __syncthreads();  // the previous item's reads of the tile are done
-        if (!transposed) {
-            // element (r, k) at src[r*ld + k]: 8 threads x 4 consecutive k per row
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int e = i * 256 + tid;
-                const int r = e >> 3, k = (e & 7) * 4;
-                const int64_t gr = r0 + r, gk = k0 + k;
-                float x[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-                if (gr < rows) {
-                    const float *ptr = src + gr * ld + gk;
-                    if (vec && gk + 3 < K) {
-                        const float4 q = __ldcs(reinterpret_cast<const float4 *>(ptr));
-                        x[0] = q.x, x[1] = q.y, x[2] = q.z, x[3] = q.w;
-                    } else {
+        for (int i = 0; i < 4; ++i) {
+            const int e = i * 256 + tid;
 #pragma unroll
-                        for (int j = 0; j < 4; ++j)
-                            if (gk + j < K) x[j] = ptr[j];
-                    }
-                }
-#pragma unroll
-                for (int j = 0; j < 4; ++j) tile[r][k + j] = x[j];
-            }
-        } else {
-            // element (r, k) at src[k*ld + r]: 32 threads x 4 consecutive rows per k
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int e = i * 256 + tid;
-                const int k = e >> 5, r = (e & 31) * 4;
-                const int64_t gr = r0 + r, gk = k0 + k;
-                float x[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-                if (gk < K) {
-                    const float *ptr = src + gk * ld + gr;
-                    if (vec && gr + 3 < rows) {
-                        const float4 q = __ldcs(reinterpret_cast<const float4 *>(ptr));
-                        x[0] = q.x, x[1] = q.y, x[2] = q.z, x[3] = q.w;
-                    } else {
-#pragma unroll
-                        for (int j = 0; j < 4; ++j)
-                            if (gr + j < rows) x[j] = ptr[j];
-                    }
-                }
-#pragma unroll
-                for (int j = 0; j < 4; ++j) tile[r + j][k] = x[j];
+            for (int j = 0; j < 4; ++j) {
+                if (!cur.transposed) tile[e >> 3][(e & 7) * 4 + j] = x[i * 4 + j];
+                else tile[(e & 31) * 4 + j][e >> 5] = x[i * 4 + j];
             }
         }
         __syncthreads();
-        uint8_t *const *dst = op ? I.pb : I.pa;
+        // next item: its loads fly while this one is split and stored
+        PackItem next = cur;
+        if (it + 1 < it1) {
+            while (it + 1 >= seg_start[sgi + 1]) ++sgi;
+            next = pack_item(insts, seg_start, sgi, it + 1);
+            pack_load(next, tid, x);
+        }
+        uint8_t *const *dst = cur.op ? cur.I->pb : cur.I->pa;
         for (int e = tid; e < kPackRows * 4; e += 256) {
             const int r = e >> 2, c = e & 3;
-            const int64_t row = r0 + r;
-            if (row >= rows_alloc) continue;
+            const int64_t row = cur.r0 + r;
+            if (row >= cur.rows_alloc) continue;
             __nv_bfloat16 pcs[8][3];
 #pragma unroll
             for (int j = 0; j < 8; ++j) tcg::split_value<NP>(tile[r][c * 8 + j], pcs[j]);
-            const int64_t off = packed_offset(row, kb, c, tr, I.kt);
+            const int64_t off = packed_offset(row, cur.kb, c, cur.tr, cur.I->kt);
 #pragma unroll
             for (int i = 0; i < NP; ++i) {
                 uint4 u;
@@ -169,6 +190,7 @@ __global__ void __launch_bounds__(256) grouped_pack_kernel(const Inst *insts, co
                 *reinterpret_cast<uint4 *>(dst[i] + off) = u;
             }
         }
+        cur = next;
     }
 }
 

@@ -216,3 +216,14 @@ def test_image_engine_empty_contraction_and_unaligned_rows(cuda):
     B = oracle.uniform(30 * N, seed=2)
     with pytest.raises(RuntimeError, match="16-byte"):
         _mm(cuda, A, B, M, N, 30, engine="image")
+
+
+@pytest.mark.parametrize("tile", [(8, 16, 8, 8, 2), (16, 8, 8, 8, 2), (8, 8, 8, 8, 2), (16, 16, 8, 8, 2), (0, 0, 0, 0, 0)],
+                         ids=lambda t: "x".join(map(str, t)))
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+def test_dgemm_points_bit_exact(cuda, tile, ta, tb):
+    M, N, K = 200, 136, 72
+    A = oracle.uniform(M * K, seed=18, dtype=np.float64)
+    B = oracle.uniform(K * N, seed=19, dtype=np.float64)
+    C = _mm(cuda, A, B, M, N, K, ta, tb, tile=tile + (0,) if any(tile) else None)
+    assert np.array_equal(C, oracle.matmul(A, B, M, N, K, ta, tb, mode=oracle.FMA, dtype=np.float64))
