@@ -631,7 +631,8 @@ def run_reference(args, rank, world):
 
 def run_case(spec: str) -> None:
     """Small single-kernel cases for ncu captures: NAME:SIZE, three calls each.
-    tc_bf16|tc_split3|tc_split6|tc_fp8:M (M^3 GEMM, prepare once, run x3), sgemm_simt:M, sgemm_image:M,
+    tc_bf16|tc_split3|tc_split6|tc_fp8[_pair]:M (M^3 GEMM, prepare once, run x3; _pair forces CTA pairs),
+    sgemm_simt:M, sgemm_image:M,
     quant_fp8:M (the FP8 operand pass, x3),
     gemv_A:N / gemv_At:N (N^2 GEMV), saxpy_buffer:n / saxpy_image:n,
     grouped_tc_split3|grouped_tc_bf16:count (the batched workload)."""
@@ -640,6 +641,10 @@ def run_case(spec: str) -> None:
     import gatlas_b200 as g
     name, size = spec.split(":")
     size = int(size)
+    if name.endswith("_pair"):  # the same case on CTA pairs (cta_group::2)
+        name = name[:-len("_pair")]
+        import gatlas_b200 as gb
+        gb.set_option("tc_pair", 2)
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     if name.startswith("tc_") or name in ("sgemm_simt", "sgemm_image", "quant_fp8"):
