@@ -123,7 +123,9 @@ class ClockSampler:
 # distributed plumbing
 # ---------------------------------------------------------------------------
 
-def _dist_init(n_gpus: int):
+def _dist_init(n_gpus: int, backend: str = "nccl"):
+    """One process per GPU: rank, world size and local rank from the launcher's
+    environment; a process group (short timeout) when world > 1."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -131,7 +133,7 @@ def _dist_init(n_gpus: int):
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return rank, world, local
 
 
@@ -142,13 +144,22 @@ def _barrier(world):
 
 
 def _max_over_ranks(x: float, world: int) -> float:
+    """Max of a per-rank time over all ranks (GPU tensor under NCCL, CPU under gloo)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def _aggregate(flops_per_rank: float, ms_per_rank: float, world: int) -> tuple[float, float]:
+    """Weak scaling: (whole-job TFLOP/s, ms_max).  Every rank does the same work;
+    the job's time is the slowest rank's."""
+    ms_max = _max_over_ranks(ms_per_rank, world)
+    return world * flops_per_rank / (ms_max * 1e-3) / 1e12, ms_max
 
 
 # ---------------------------------------------------------------------------
@@ -416,9 +427,8 @@ def run_ours(args, rank, world, local):
     sampler.start()
     ms = _timed(step, args.steps, args.warmup, world, stream)
     clocks = sampler.stop()
-    ms_max = _max_over_ranks(ms, world)
     flops = 2.0 * M * N * K
-    value = world * flops / (ms_max * 1e-3) / 1e12
+    value, ms_max = _aggregate(flops, ms, world)
     fro, refn, mx, _ = g.residual(A, B, C, M, N, K)
 
     # dominant kernel alone: the tcgen05 contraction on prepared operands
