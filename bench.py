@@ -63,19 +63,58 @@ FP32_SIMT_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """Samples the SM clock, power and clock-event (throttle) reasons of one GPU
+    every 10 ms through NVML while the timed region runs; falls back to
+    `nvidia-smi -lms 200` where NVML is unavailable."""
 
+    # NVML clock-event reason bits (nvml.h)
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown"}
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device_index: int):
         self.dev = device_index
+        self.samples: list[tuple[float, float, int]] = []  # (sm MHz, W, reason bits)
+        self.smax = None
+        self._stop = threading.Event()
+        self._t = None
         self.proc = None
         self.lines: list[str] = []
-        self._t = None
+        self.nvml = None
+
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID("GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.dev)
 
     def start(self):
+        try:
+            nv, h = self._handle()
+            self.nvml = (nv, h)
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+
+            def poll():
+                while not self._stop.is_set():
+                    try:
+                        self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                             nv.nvmlDeviceGetPowerUsage(h) / 1000.0, int(reasons(h))))
+                    except Exception:
+                        pass
+                    self._stop.wait(0.01)
+            self._t = threading.Thread(target=poll, daemon=True)
+            self._t.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
@@ -84,14 +123,23 @@ class ClockSampler:
         except OSError:
             self.proc = None
             return
-        self._t = threading.Thread(target=self._read, daemon=True)
+        self._t = threading.Thread(target=lambda: self.lines.extend(ln.strip() for ln in self.proc.stdout),
+                                   daemon=True)
         self._t.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def stop(self) -> dict:
+        if self.nvml is not None:
+            self._stop.set()
+            if self._t:
+                self._t.join(timeout=2)
+            sm = [x[0] for x in self.samples]
+            bits = 0
+            for x in self.samples:
+                bits |= x[2]
+            reasons = sorted(nm for b, nm in self.REASONS.items() if bits & b)
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.smax,
+                    "reasons": reasons, "samples": len(sm),
+                    "power_w_max": max((x[1] for x in self.samples), default=None), "source": "nvml, 10 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -116,7 +164,7 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 # ---------------------------------------------------------------------------
@@ -171,7 +219,7 @@ PRODUCTS = {"tc_bf16": 1, "tc_split3": 3, "tc_split6": 6}
 SWEEP_ENGINES = ("buffer", "tc_bf16", "tc_split3", "tc_split6", "tc_fp8")
 
 
-def _timed(fn, steps, warmup, world, stream):
+def _timed(fn, steps, warmup, world, stream, sampler=None):
     import torch
     for _ in range(warmup):
         fn()
@@ -180,11 +228,15 @@ def _timed(fn, steps, warmup, world, stream):
     torch.cuda.synchronize()
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
+    if sampler is not None:
+        sampler.start()  # samples exactly the timed launches
     start.record(stream)
     for _ in range(steps):
         fn()
     stop.record(stream)
     torch.cuda.synchronize()
+    if sampler is not None:
+        sampler.clocks = sampler.stop()
     _barrier(world)
     return start.elapsed_time(stop) / steps  # ms per step
 
@@ -424,9 +476,8 @@ def run_ours(args, rank, world, local):
     launches_per_step = 1 if engine == "buffer" else 3     # split A, split B, contraction
 
     sampler = ClockSampler(local)
-    sampler.start()
-    ms = _timed(step, args.steps, args.warmup, world, stream)
-    clocks = sampler.stop()
+    ms = _timed(step, args.steps, args.warmup, world, stream, sampler=sampler)
+    clocks = sampler.clocks
     flops = 2.0 * M * N * K
     value, ms_max = _aggregate(flops, ms, world)
     fro, refn, mx, _ = g.residual(A, B, C, M, N, K)

@@ -1,6 +1,7 @@
-"""bench.py across processes on CPU: two ranks over gloo (127.0.0.1) take the
+"""bench.py host plumbing on CPU: two ranks over gloo (127.0.0.1) take the
 barrier, reduce their step times to the slowest rank's and report whole-job
-throughput for weak scaling; under --impl reference only rank 0 works."""
+throughput for weak scaling; under --impl reference only rank 0 works; the
+clock sampler reports even where no GPU can be queried."""
 import json
 import os
 import socket
@@ -56,3 +57,13 @@ def test_single_process_needs_no_process_group():
     import bench
     assert bench._aggregate(2e12, 4.0, 1) == (pytest.approx(500.0), 4.0)
     bench._barrier(1)
+
+
+def test_clock_sampler_reports_without_a_gpu():
+    # with neither NVML nor nvidia-smi usable the sampler says so instead of failing
+    sys.path.insert(0, ROOT)
+    import bench
+    s = bench.ClockSampler(0)
+    s.start()
+    out = s.stop()
+    assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(out)
