@@ -246,14 +246,18 @@ int32_t gatlas_grouped_bucket(int64_t m, int64_t n, int64_t k);
 int gatlas_grouped_set_tile_table(int engine, const int32_t *bucket_tile_n, int32_t nbuckets);
 int gatlas_grouped_get_tile_table(int engine, int32_t *bucket_tile_n, int32_t nbuckets);
 
-/* Autotunes the tile width of every bucket: a seeded synthetic group of 48
- * instances per bucket (m, k log-uniform in [16,4096], n log-uniform in the
- * bucket, multiples of 16, random layouts) is timed over `trials` runs at
- * each width 64/128/256; the fastest width goes into the table (and into
- * out_table when not NULL).  Every candidate is recorded in the journal at
- * journal_path (NULL or "": none) with the reference's run states
- * (GatlasBenchmark.cpp:185-288) under the key "grouped<engine>_<bucket>_
- * <width>_48_<seed>_"; recorded times are replayed, crashed ones skipped. */
+/* Autotunes the tile width of every bucket.  One seeded synthetic group
+ * holds 48 instances per bucket (m, k log-uniform in [16,4096], n
+ * log-uniform in the bucket, multiples of 16, random layouts).  Bucket by
+ * bucket, the whole group is timed over `trials` runs with that bucket at
+ * each width 64/128/256 and the others at their current widths, and the
+ * fastest width stays (a width pays off or not beside the other buckets'
+ * work).  The final table is installed (and copied to out_table when not
+ * NULL).  Every timing is recorded in the journal at journal_path (NULL or
+ * "": none) with the reference's run states (GatlasBenchmark.cpp:185-288)
+ * under the key "grouped<engine>_<bucket>_<width>_192_<seed>_<t0>_<t1>_<t2>_
+ * <t3>_" (t = the table timed); recorded times are replayed, crashed ones
+ * skipped. */
 int gatlas_grouped_autotune(int engine, const char *journal_path, int32_t trials, uint64_t seed,
                             int32_t *out_table);
 

@@ -133,11 +133,14 @@ def test_autotune_journals_and_replays(cuda, tmp_path):
         table = g.grouped_autotune("tc_bf16", journal=str(j), trials=1, seed=3)
         assert all(t in (64, 128, 256) for t in table)
         lines = [ln.split("\t") for ln in j.read_text().splitlines()]
-        assert len(lines) == 4 * 3 * 5
+        assert len(lines) % 5 == 0 and 4 * 2 * 5 <= len(lines) <= 4 * 3 * 5   # a repeated table is replayed
         assert [int(v) for _, v in lines[:4]] == [BUILD_IN_PROGRESS, BUILD_OK, RUN_IN_PROGRESS, RUN_OK]
-        assert lines[0][0] == "groupedtcbf16_0_64_48_3_"
-        # resumed: every candidate replayed from the journal, same decision
+        t0 = old
+        assert lines[0][0] == "groupedtcbf16_0_64_192_3_64_%d_%d_%d_" % tuple(t0[1:])
+        # resumed: every timing replayed from the journal, same decision
+        n = len(lines)
+        g.grouped_tile_table("tc_bf16", old)
         assert g.grouped_autotune("tc_bf16", journal=str(j), trials=1, seed=3) == table
-        assert len(j.read_text().splitlines()) == 60
+        assert len(j.read_text().splitlines()) == n
     finally:
         g.grouped_tile_table("tc_bf16", old)
