@@ -115,6 +115,7 @@ def lib() -> ctypes.CDLL:
     L.gatlas_device_faults.argtypes = [ctypes.POINTER(ctypes.c_int), i32]
     L.gatlas_matmul_f32_host.argtypes = [ctypes.POINTER(MatmulDesc), vp, vp, vp, vp]
     L.gatlas_set_option.argtypes = [ctypes.c_char_p, ctypes.c_int64]
+    L.gatlas_selftest_bounded_wait.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.POINTER(ctypes.c_int), vp]
     L.gatlas_get_option.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
     gi = ctypes.POINTER(GroupedInstance)
     L.gatlas_grouped_workspace_size.argtypes = [i32, gi, ctypes.c_int32]
@@ -516,3 +517,15 @@ def matmul_host(A, B, M, N, K, C, trans_a=False, trans_b=False, gemm=False, alph
                     tile=(0, 0, 0, 0, 0, extra))
     check(lib().gatlas_matmul_f32_host(ctypes.byref(d), _ptr(A), _ptr(B), _ptr(C), _stream(stream)))
     return C
+
+
+FAULT_SELFTEST_WAIT = 1 << 6
+
+
+def selftest_bounded_wait(limit_ns=1_000_000, arrive=False, stream=None) -> bool:
+    """Runs the bounded mbarrier wait every TMA kernel uses; True when the wait
+    completed, False when it ran out (and set FAULT_SELFTEST_WAIT)."""
+    done = ctypes.c_int(-1)
+    s = None if stream is None else _stream(stream)  # NULL: the legacy default stream
+    check(lib().gatlas_selftest_bounded_wait(int(limit_ns), int(bool(arrive)), ctypes.byref(done), s))
+    return done.value == 1

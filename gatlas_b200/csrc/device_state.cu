@@ -98,3 +98,55 @@ extern "C" int gatlas_set_device(int device) {
     if (e != cudaSuccess) return gatlas::set_error(GATLAS_ERR_CUDA, "cudaSetDevice(%d): %s", device, cudaGetErrorString(e));
     return GATLAS_OK;
 }
+
+// ---------------------------------------------------------------------------
+// bounded-wait self-test
+// ---------------------------------------------------------------------------
+namespace gatlas {
+namespace {
+
+// One thread waits on an mbarrier in the way every TMA/tcgen05 kernel here
+// does: try_wait polls bounded by `limit_ns` of wall time.  With `arrive` the
+// barrier's phase completes first and the wait succeeds; without it nothing
+// ever completes the phase, the wait runs out, the fault word gets its bit and
+// the kernel returns.
+__global__ void selftest_wait_kernel(int *fault, uint64_t limit_ns, int arrive, int *result) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    fence_mbarrier_init();
+    if (arrive) mbar_arrive(&bar);
+    uint64_t t0;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    bool ok = false;
+    while (true) {
+        if (mbar_try_wait(&bar, 0)) {
+            ok = true;
+            break;
+        }
+        uint64_t t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (t - t0 > limit_ns) break;
+    }
+    if (!ok) report_fault(fault, kFaultSelftestWait);
+    *result = ok ? 1 : 0;
+}
+
+}  // namespace
+}  // namespace gatlas
+
+extern "C" int gatlas_selftest_bounded_wait(int64_t limit_ns, int arrive, int *completed, void *stream) {
+    using namespace gatlas;
+    if (limit_ns <= 0 || limit_ns > 2000000000LL || !completed)
+        return set_error(GATLAS_ERR_INVALID, "selftest: limit must be in (0, 2 s] and `completed` non-null");
+    int *fault = device_fault_word();
+    int *res = static_cast<int *>(device_scratch(sizeof(int), 1));
+    if (!fault || !res) return set_error(GATLAS_ERR_NOMEM, "selftest: device words");
+    selftest_wait_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(fault, (uint64_t)limit_ns, arrive, res);
+    int rc = check_launch("selftest_wait_kernel");
+    if (rc) return rc;
+    if (cudaMemcpyAsync(completed, res, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream) != cudaSuccess ||
+        cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess)
+        return check_launch("selftest result");
+    return GATLAS_OK;
+}

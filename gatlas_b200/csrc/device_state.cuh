@@ -15,6 +15,7 @@ enum FaultCode : int {
     kFaultTcProducerWait = 1 << 3,
     kFaultTcMmaWait = 1 << 4,
     kFaultTcEpilogueWait = 1 << 5,
+    kFaultSelftestWait = 1 << 6,
 };
 
 // Device pointer to the current device's fault word (allocated and zeroed on

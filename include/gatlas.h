@@ -76,7 +76,11 @@ int gatlas_saxpy_f64(int engine, size_t n, double alpha, const double *x, const 
  * KernelMatvecImage.hpp:188-295).  Deterministic: the summation order
  * depends only on (M, N, engine) and the device's SM count.
  * `workspace` may be NULL, in which case the library uses an internal
- * per-device buffer; gatlas_matvec_workspace_size() gives the bytes needed. */
+ * per-device buffer; gatlas_matvec_workspace_size() gives the bytes needed.
+ * Calls that use the internal per-device buffers (here, gatlas_matmul_* with
+ * no workspace, gatlas_matmul_f32_host) share them: calls on one device that
+ * overlap on the GPU (several streams or host threads) race; serialise them or
+ * pass workspaces. */
 typedef struct gatlas_matvec_desc {
     int32_t engine;  /* GATLAS_ENGINE_BUFFER or GATLAS_ENGINE_IMAGE */
     int32_t gemv;
@@ -385,6 +389,14 @@ int gatlas_set_device(int device);
  * clears it when `clear` is non-zero.  No reference counterpart (the
  * reference detects hangs only through its journal, GatlasBenchmark.cpp:178-289). */
 int gatlas_device_faults(int *flags, int clear);
+
+/* Exercises that mechanism without a fault: one thread waits on an mbarrier
+ * with the library's bounded poll, limited to limit_ns (at most 2 s).  With
+ * arrive != 0 the phase completes first and *completed = 1; with arrive == 0
+ * nothing completes it, the wait runs out, the fault word gets bit 6 (1 << 6)
+ * and *completed = 0, and the device stays usable.  Synchronises `stream`.
+ * No reference counterpart. */
+int gatlas_selftest_bounded_wait(int64_t limit_ns, int arrive, int *completed, void *stream);
 
 #ifdef __cplusplus
 }
