@@ -962,15 +962,15 @@ static WsPtrs ws_ptrs(const Plan &pl, void *ws) {
 }
 
 // CTA pairs (256 x 256 tiles) for M > 128: 1 = where they measure faster on
-// B200 (the six-product engine: 264 vs 239 TFLOP/s at 8192^3; BF16, split3
-// and FP8 run faster as single CTAs), 2 = always, 0 = never.
+// B200 (the split engines: at 8192^3 split3 491 vs 476 and split6 257 vs 242
+// TFLOP/s; BF16 and FP8 run faster as single CTAs), 2 = always, 0 = never.
 static int g_tc_pair = 1;
 
 template <int MODE>
 static int launch_tc(const Geometry &g, const Plan &pl, const WsPtrs &w, float *C, double alpha, double beta,
                      int gemm, int seg_kblocks, cudaStream_t stream) {
     using L = Layout<MODE>;
-    const bool pair = g.M > BM && (g_tc_pair == 2 || (g_tc_pair == 1 && MODE == 2));
+    const bool pair = g.M > BM && (g_tc_pair == 2 || (g_tc_pair == 1 && (MODE == 1 || MODE == 2)));
     CUtensorMap ta[3], tb[3];
     const uint64_t row_bytes = (uint64_t)pl.Kp * pl.elem;
     const uint64_t adims[3] = {(uint64_t)pl.Kp, (uint64_t)g.M, (uint64_t)g.batch};

@@ -50,6 +50,13 @@ constexpr int kThreads = 32 * (2 + kDrainWarps);
 constexpr uint32_t kTmemCols = 512;       // two accumulators of up to 256 columns
 constexpr uint64_t kWaitNs = 2000000000ull;
 constexpr int kPackRows = 128;            // rows per pack item
+// The grouped engine stages 64-byte K slices (its packed tiles carry the
+// 64-byte swizzle) and promotes after the same K as the single-instance
+// engine (512 for one-product BF16, 128 for split3), issuing the same MMA
+// sequence, so that each instance's result is bit-identical to it.
+template <int MODE>
+using GLayout = tcg::Layout<MODE, kRowBytes>;
+constexpr int grouped_seg_kblocks(int mode) { return mode == 0 ? 16 : 4; }
 
 // Packed byte offset of 16-byte chunk c of row `row` in K slice kb.
 __device__ __forceinline__ int64_t packed_offset(int64_t row, int kb, int c, int tr, int kt) {
@@ -206,10 +213,10 @@ struct Params {
 
 template <int MODE>
 __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
-    using L = tcg::Layout<MODE>;
+    using L = GLayout<MODE>;
     using MD = tcg::Mode<MODE>;
     constexpr int S = L::STAGES;
-    static_assert(L::ROW_BYTES == kRowBytes, "grouped engine stages BF16 slices of 32");
+    static_assert(L::BK == kBK, "grouped engine stages BF16 slices of 32");
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     __shared__ __align__(8) uint64_t full[S], empty[S], tfull[2], tempty[2], mma_done;
@@ -627,11 +634,11 @@ int grouped_launch_pack(const GroupedTables &t, const GroupedDevice &d, cudaStre
 
 template <int MODE>
 static int launch_grouped(const GroupedTables &t, const GroupedDevice &d, cudaStream_t stream) {
-    using L = tcg::Layout<MODE>;
+    using L = grp::GLayout<MODE>;
     grp::Params prm;
     prm.tiles = d.tiles;
     prm.cta_start = d.cta;
-    prm.seg_kblocks = tcg::default_seg_kblocks(MODE);
+    prm.seg_kblocks = grp::grouped_seg_kblocks(MODE);
     prm.fault = device_fault_word();
     const int smem = (int)L::SMEM_BYTES;
     static thread_local int attr_set[2] = {-1, -1};  // device whose attribute was set
@@ -790,9 +797,9 @@ int grouped_launch_graph(GroupedPlan *p, int with_prepare, cudaStream_t stream) 
             return set_error(GATLAS_ERR_CUDA, "grouped: capture stream");
         // attribute changes are not captured: set them before the capture
         cudaFuncSetAttribute(grp::grouped_gemm_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)tcg::Layout<0>::SMEM_BYTES);
+                             (int)grp::GLayout<0>::SMEM_BYTES);
         cudaFuncSetAttribute(grp::grouped_gemm_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)tcg::Layout<1>::SMEM_BYTES);
+                             (int)grp::GLayout<1>::SMEM_BYTES);
         device_fault_word();
         cudaGraph_t graph = nullptr;
         int rc = GATLAS_OK;

@@ -12,37 +12,40 @@ namespace tcg {
 
 constexpr int BM = 128, BN = 256;
 
-// Default promotion interval for the BF16 modes: 4 slices of 32, i.e.
-// K = 128 per TMEM segment (selectable per call through the descriptor's
-// extra field).  The FP8 mode promotes every slice (one scale block).
-constexpr int kDefaultSegKblocks = 4;
-// One-product BF16 promotes every 16 slices (K = 512): its MMA segment of 4
-// slices is shorter than the drain, and the longer TMEM accumulation adds
-// nothing measurable next to BF16's own input rounding (2^-9).
-constexpr int kDefaultSegKblocksBf16 = 16;
+// Default promotion intervals, in K slices of each mode (selectable per call
+// through the descriptor's extra field): the split modes promote every
+// K = 128 (2 slices of 64 for split3, 4 of 32 for split6).  One-product BF16
+// promotes every K = 512 (8 slices): a shorter MMA segment would be shorter
+// than the drain, and the longer TMEM accumulation adds nothing measurable
+// next to BF16's own input rounding (2^-9).  FP8 accumulates runs of at most
+// 4 equally scaled 128-deep blocks.
 __host__ __device__ constexpr int default_seg_kblocks(int mode) {
-    return mode == 0 ? kDefaultSegKblocksBf16 : kDefaultSegKblocks;
+    return mode == 0 ? 8 : (mode == 1 ? 2 : 4);
 }
-// FP8: most 128-deep blocks per tile (K <= 131072), and by default at most
-// 4 equally scaled blocks accumulate in TMEM before promotion.
+// FP8: most 128-deep blocks per tile (K <= 131072).
 constexpr int kMaxFp8Blocks = 1024;
 
 // MODE 0: one BF16 piece, one product; 1: two pieces, three products;
 // 2: three pieces, six products; 3: FP8 E4M3 codes with one FP32 scale per
-// 128 x 128 block of each operand.  Every mode stages K slices of 32 bytes
-// per MMA instruction: K = 16 BF16 or K = 32 E4M3 elements.
+// 128 x 128 block of each operand.  Each MMA instruction consumes 32 bytes
+// of K per row (K = 16 BF16 or K = 32 E4M3 elements); a pipeline slice is
+// one ROWB-byte row per operand row: 128 bytes (128-byte swizzle) where the
+// ring still holds at least two slices, 64 bytes (64-byte swizzle) for the
+// six-product mode, whose three pieces per operand would leave one.  On
+// B200 the tensor core streams 128-byte-swizzled rows markedly faster: the
+// one-product BF16 kernel runs 993 instead of 630 TFLOP/s at 8192^3.
 template <int MODE>
 struct Mode;
 template <>
 struct Mode<0> {
-    static constexpr int NP = 1, NPROD = 1, STAGES = 8, ELEM = 2, BKE = 32;
+    static constexpr int NP = 1, NPROD = 1, ELEM = 2, ROWB = 128;
     static constexpr bool SCALED = false;
     __device__ static constexpr int pa(int) { return 0; }
     __device__ static constexpr int pb(int) { return 0; }
 };
 template <>
 struct Mode<1> {
-    static constexpr int NP = 2, NPROD = 3, STAGES = 4, ELEM = 2, BKE = 32;
+    static constexpr int NP = 2, NPROD = 3, ELEM = 2, ROWB = 128;
     static constexpr bool SCALED = false;
     // hi*hi, hi*lo, lo*hi
     __device__ static constexpr int pa(int j) { return j == 2 ? 1 : 0; }
@@ -50,7 +53,7 @@ struct Mode<1> {
 };
 template <>
 struct Mode<2> {
-    static constexpr int NP = 3, NPROD = 6, STAGES = 3, ELEM = 2, BKE = 32;
+    static constexpr int NP = 3, NPROD = 6, ELEM = 2, ROWB = 64;
     static constexpr bool SCALED = false;
     // hi*hi, hi*mid, mid*hi, mid*mid, hi*lo, lo*hi
     __device__ static constexpr int pa(int j) { return j == 2 || j == 3 ? 1 : (j == 5 ? 2 : 0); }
@@ -58,19 +61,20 @@ struct Mode<2> {
 };
 template <>
 struct Mode<3> {
-    static constexpr int NP = 1, NPROD = 1, STAGES = 4, ELEM = 1, BKE = 128;
+    static constexpr int NP = 1, NPROD = 1, ELEM = 1, ROWB = 128;
     static constexpr bool SCALED = true;
     __device__ static constexpr int pa(int) { return 0; }
     __device__ static constexpr int pb(int) { return 0; }
 };
 
-template <int MODE>
+// Single-CTA layout (128 x 256 tiles) with ROWB-byte K slices; the ring
+// takes as many stages as 226 KB of shared memory hold, at most 8.
+template <int MODE, uint32_t ROWB = Mode<MODE>::ROWB>
 struct Layout {
     using MD = Mode<MODE>;
     static constexpr int NP = MD::NP;
-    static constexpr int STAGES = MD::STAGES;
-    static constexpr int BK = MD::BKE;                              // elements per K slice
-    static constexpr uint32_t ROW_BYTES = BK * MD::ELEM;            // 64 (BF16) or 128 (FP8)
+    static constexpr uint32_t ROW_BYTES = ROWB;                     // 64 or 128
+    static constexpr int BK = (int)(ROWB / MD::ELEM);               // elements per K slice
     static constexpr uint32_t SWIZZLE = ROW_BYTES == 128 ? tc::kSwizzle128B : tc::kSwizzle64B;
     static constexpr uint32_t SBO = 8 * ROW_BYTES;                  // 8-row core-matrix groups
     static constexpr uint32_t A_TILE = BM * ROW_BYTES;
@@ -80,6 +84,11 @@ struct Layout {
     // FP8: per-block scale products of the tile's two column halves, compacted
     // in place into per-segment scales, and one segment-start flag per block
     static constexpr uint32_t PLAN_BYTES = MD::SCALED ? (2 * 4 + 1) * 1024 : 0;
+    static constexpr uint32_t BUDGET = 226 * 1024;
+    static constexpr int FIT = (int)((BUDGET - PLAN_BYTES - 1024) / STAGE_BYTES);
+    static constexpr int STAGES = FIT < 8 ? FIT : 8;
+    static_assert(STAGES >= 2, "tensor-core pipeline depth");
+    static_assert(ROWB == 64 || ROWB == 128, "K slice of 64 or 128 bytes");
     static constexpr uint32_t SMEM_BYTES = STAGES * STAGE_BYTES + PLAN_BYTES + 1024;  // + alignment slack
     static constexpr uint32_t IDESC = MD::SCALED ? tc::idesc_e4m3_f32(BM, BN) : tc::idesc_bf16_f32(BM, BN);
 };

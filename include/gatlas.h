@@ -133,9 +133,10 @@ int gatlas_matvec_f32_noalloc(const gatlas_matvec_desc *d, const float *A, const
  * SIMT engines accumulate k = 0..K-1 as one fused multiply-add chain per
  * element, bit-exact against a sequential fmaf chain.  For the TC_* engines
  * the tile fields are ignored and `extra` is the promotion interval: the
- * tensor cores accumulate `extra` slices of K = 32 in TMEM before the partial
- * sum is added into round-to-nearest FP32 registers (0 selects 4, K = 128;
- * 16, K = 512, for the one-product BF16 engine).
+ * tensor cores accumulate `extra` K slices in TMEM before the partial sum is
+ * added into round-to-nearest FP32 registers.  A slice is K = 64 for TC_BF16
+ * and TC_SPLIT3 and K = 32 for TC_SPLIT6; 0 selects K = 128 (K = 512 for the
+ * one-product BF16 engine).
  * GATLAS_ENGINE_TC_FP8 quantises each operand to E4M3 with one power-of-two
  * FP32 scale per 128 x 128 block (the smallest power of two s with
  * amax / s <= 448); runs of up to `extra` (0 selects 4) 128-deep blocks
@@ -189,7 +190,7 @@ int gatlas_matmul_f32_host(const gatlas_matmul_desc *d, const float *A, const fl
 /* Library options.  "tc_pair": whether tensor-core contractions with
  * M > 128 run as CTA pairs (cta_group::2, a 256 x 256 tile per pair, each
  * CTA staging half of B) or one CTA per 128 x 256 tile: 1 (default) where
- * pairs measure faster (the six-product engine), 2 always, 0 never.  Results
+ * pairs measure faster (the split3 and split6 engines), 2 always, 0 never.  Results
  * are bit-identical either way (same pieces, same MMA order, same
  * promotion). */
 int gatlas_set_option(const char *name, int64_t value);
