@@ -150,6 +150,16 @@ __device__ __forceinline__ void tma_load_3d(void *smem_dst, const void *tmap, in
         : "memory");
 }
 
+// 3-D tiled tensor copy of this CTA's shared memory to global memory,
+// tracked by bulk async-groups; elements outside the tensor are not written.
+// x * element size must be a multiple of 16 bytes and no coordinate negative.
+__device__ __forceinline__ void tma_store_3d(const void *tmap, const void *smem_src, int32_t x, int32_t y,
+                                             int32_t z) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(tmap),
+                 "r"(x), "r"(y), "r"(z), "r"(smem_u32(smem_src))
+                 : "memory");
+}
+
 __device__ __forceinline__ void prefetch_tmap(const void *tmap) {
     asm volatile("prefetch.tensormap [%0];" ::"l"(tmap) : "memory");
 }

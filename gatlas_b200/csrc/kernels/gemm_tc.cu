@@ -55,6 +55,10 @@ struct Params {
     int64_t scale_a_stride, scale_b_stride;  // per instance
     int nblocks_n;                           // 128-column blocks of N
     int nblocks_m;                           // 128-row blocks of M
+    // persistent kernels: tiles per instance and instances; tma_store = 1
+    // when C leaves through the C tensor map (beta == 0, 16-byte aligned)
+    int tiles_m, tiles_n, batch;
+    int tma_store;
 };
 
 // Warp roles: warp 0 = TMA producer (lane 0), warp 1 = MMA issuer (lane 0),
@@ -655,6 +659,336 @@ __global__ void __launch_bounds__(kThreads2, 1)
 }
 
 // ---------------------------------------------------------------------------
+// Persistent contraction (BF16 modes): one CTA (or CTA pair) per SM walks
+// the tiles t = unit, unit + units, ... in the grouped raster order.  The
+// ring, the MMA issue and the TMEM double buffer run on across tile
+// boundaries, so one tile's last promotions and its C stores overlap the
+// next tile's loads and MMAs; each drain warp stages its 32 x 128 block of C
+// through a 32 x 32 shared-memory tile (128-byte swizzle) and a TMA store,
+// which also clips the tile at M and N.  PAIR as in tc_gemm_pair_kernel.
+// ---------------------------------------------------------------------------
+template <int MODE, bool PAIR>
+__global__ void __launch_bounds__(kThreads2, 1)
+    tc_gemm_persistent_kernel(const __grid_constant__ CUtensorMap ta0, const __grid_constant__ CUtensorMap ta1,
+                              const __grid_constant__ CUtensorMap ta2, const __grid_constant__ CUtensorMap tb0,
+                              const __grid_constant__ CUtensorMap tb1, const __grid_constant__ CUtensorMap tb2,
+                              const __grid_constant__ CUtensorMap tcout, Params p) {
+    using L = PersistentLayout<MODE, PAIR>;
+    using MD = Mode<MODE>;
+    constexpr int S = L::STAGES;
+    constexpr int BK = L::BK;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    __shared__ __align__(8) uint64_t full[S], empty[S], tfull[2], tempty[2], mma_done;
+    __shared__ uint32_t tmem_base;
+    __shared__ volatile int abort_flag;
+    __shared__ int mma_aborted;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = PAIR ? tc::cluster_ctarank() : 0u;
+    const bool leader = rank == 0;
+    const int unit = PAIR ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
+    const int units = PAIR ? (int)(gridDim.x >> 1) : (int)gridDim.x;
+    const int64_t per_batch = (int64_t)p.tiles_m * p.tiles_n;
+    const int64_t total = per_batch * p.batch;
+    const CUtensorMap *tA[3] = {&ta0, &ta1, &ta2};
+    const CUtensorMap *tB[3] = {&tb0, &tb1, &tb2};
+
+    // tile t -> (tile row, tile column, instance), grouped raster within an instance
+    auto decode = [&](int64_t t, int &tm, int &tn, int &z) {
+        z = (int)(t / per_batch);
+        const int bid = (int)(t - (int64_t)z * per_batch);
+        const int per_group = kGroupM * p.tiles_n;
+        const int first_m = (bid / per_group) * kGroupM;
+        const int gm = min(p.tiles_m - first_m, kGroupM);
+        const int r = bid % per_group;
+        tm = first_m + r % gm;
+        tn = r / gm;
+    };
+    auto wait = [&](uint64_t *bar, uint32_t parity, uint64_t limit) {
+        return PAIR ? tc::wait_timed_cluster(bar, parity, limit, &abort_flag)
+                    : tc::wait_timed(bar, parity, limit, &abort_flag);
+    };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], (PAIR ? 2 : 1) * kDrainWarps);
+        }
+        mbar_init(&mma_done, 1);
+        fence_mbarrier_init();
+        abort_flag = 0;
+        mma_aborted = 0;
+        for (int i = 0; i < MD::NP; ++i) {
+            prefetch_tmap(tA[i]);
+            prefetch_tmap(tB[i]);
+        }
+        if (p.tma_store) prefetch_tmap(&tcout);
+    }
+    if (warp == 0) {
+        if constexpr (PAIR) {
+            tc::tmem_alloc_pair(&tmem_base, kTmemCols2);
+            tc::tmem_relinquish_pair();
+        } else {
+            tc::tmem_alloc(&tmem_base, kTmemCols2);
+            tc::tmem_relinquish();
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if constexpr (PAIR) tc::cluster_sync();  // both CTAs' barriers exist before any signal crosses the pair
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_base;
+
+    auto a_tile = [&](int s, int piece) { return smem + s * L::STAGE_BYTES + piece * L::A_TILE; };
+    auto b_tile = [&](int s, int piece) { return smem + s * L::STAGE_BYTES + MD::NP * L::A_TILE + piece * L::B_TILE; };
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---- TMA producer: one ring position per K slice, across tiles ----
+            const uint32_t full_leader = PAIR ? tc::mapa_shared(smem_u32(&full[0]), 0) : 0u;
+            int s = 0;
+            uint32_t ph = 0;
+            bool stop = false;
+            for (int64_t t = unit; t < total && !stop; t += units) {
+                int tm, tn, z;
+                decode(t, tm, tn, z);
+                const int m0 = tm * L::TM + (int)rank * 128;
+                const int nb = tn * BN + (int)rank * (PAIR ? 128 : 0);
+                for (int kb = 0; kb < p.kblocks; ++kb) {
+                    if (!wait(&empty[s], ph ^ 1u, kWaitNs)) {
+                        if (!abort_flag) report_fault(p.fault, kFaultTcProducerWait);
+                        abort_flag = 1;
+                        stop = true;
+                        break;
+                    }
+                    if constexpr (PAIR) {
+                        if (leader) mbar_arrive_expect_tx(&full[s], 2 * L::STAGE_BYTES);
+                        const uint32_t bar = full_leader + (uint32_t)(s * sizeof(uint64_t));
+                        for (int i = 0; i < MD::NP; ++i) {
+                            tc::tma_load_3d_pair(a_tile(s, i), tA[i], kb * BK, m0, z, bar);
+                            tc::tma_load_3d_pair(b_tile(s, i), tB[i], kb * BK, nb, z, bar);
+                        }
+                    } else {
+                        mbar_arrive_expect_tx(&full[s], L::STAGE_BYTES);
+                        for (int i = 0; i < MD::NP; ++i) {
+                            tma_load_3d(a_tile(s, i), tA[i], kb * BK, m0, z, &full[s]);
+                            tma_load_3d(b_tile(s, i), tB[i], kb * BK, nb, z, &full[s]);
+                        }
+                    }
+                    if (++s == S) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0 && leader) {
+            // ---- MMA issuer: segment g (counted across tiles) accumulates into TMEM buffer g & 1 ----
+            constexpr uint32_t idesc = L::IDESC;
+            const uint32_t empty_self = PAIR ? tc::mapa_shared(smem_u32(&empty[0]), 0) : 0u;
+            const uint32_t empty_peer = PAIR ? tc::mapa_shared(smem_u32(&empty[0]), 1) : 0u;
+            const uint32_t tfull_self = PAIR ? tc::mapa_shared(smem_u32(&tfull[0]), 0) : 0u;
+            const uint32_t tfull_peer = PAIR ? tc::mapa_shared(smem_u32(&tfull[0]), 1) : 0u;
+            int s = 0, seg = -1;
+            uint32_t ph = 0;
+            bool stop = false;
+            for (int64_t t = unit; t < total && !stop; t += units) {
+                for (int kb = 0; kb < p.kblocks; ++kb) {
+                    const bool seg_first = (kb % p.seg_kblocks) == 0;
+                    const bool seg_last = (kb % p.seg_kblocks) == p.seg_kblocks - 1 || kb == p.kblocks - 1;
+                    if (seg_first) ++seg;
+                    const int b = seg & 1;
+                    if (seg_first) {
+                        // the drain of this buffer's previous segment (both CTAs' for a pair) is done
+                        if (!wait(&tempty[b], ((uint32_t)(seg >> 1) & 1u) ^ 1u, kWaitNs)) {
+                            if (!abort_flag) report_fault(p.fault, kFaultTcMmaWait);
+                            abort_flag = 1;
+                            stop = true;
+                            break;
+                        }
+                        tc::fence_after_sync();
+                    }
+                    if (!wait(&full[s], ph, kWaitNs)) {
+                        if (!abort_flag) report_fault(p.fault, kFaultTcMmaWait);
+                        abort_flag = 1;
+                        stop = true;
+                        break;
+                    }
+                    tc::fence_after_sync();
+                    const uint32_t d = tmem + (uint32_t)(b * BN);
+#pragma unroll
+                    for (int kk = 0; kk < L::KSTEPS; ++kk) {
+#pragma unroll
+                        for (int j = 0; j < MD::NPROD; ++j) {
+                            // 32 bytes of K per instruction inside the swizzled rows
+                            const uint32_t a_addr = smem_u32(a_tile(s, MD::pa(j))) + kk * 32;
+                            const uint32_t b_addr = smem_u32(b_tile(s, MD::pb(j))) + kk * 32;
+                            const uint64_t ad = tc::smem_desc_kmajor(a_addr, L::SBO, L::SWIZZLE);
+                            const uint64_t bd = tc::smem_desc_kmajor(b_addr, L::SBO, L::SWIZZLE);
+                            const uint32_t accum = (seg_first && kk == 0 && j == 0) ? 0u : 1u;
+                            if constexpr (PAIR) tc::mma_bf16_pair(d, ad, bd, idesc, accum);
+                            else tc::mma_bf16(d, ad, bd, idesc, accum);
+                        }
+                    }
+                    if constexpr (PAIR) {
+                        const uint32_t so = (uint32_t)(s * sizeof(uint64_t)), bo = (uint32_t)(b * sizeof(uint64_t));
+                        tc::commit_pair_to(empty_self + so);
+                        tc::commit_pair_to(empty_peer + so);
+                        if (seg_last) {
+                            tc::commit_pair_to(tfull_self + bo);
+                            tc::commit_pair_to(tfull_peer + bo);
+                        }
+                    } else {
+                        tc::commit_to(&empty[s]);
+                        if (seg_last) tc::commit_to(&tfull[b]);
+                    }
+                    if (++s == S) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+            }
+            if (stop) {
+                // every MMA issued before the abort completes before TMEM is freed
+                mma_aborted = 1;
+                if constexpr (PAIR) tc::commit_pair_to(tc::mapa_shared(smem_u32(&mma_done), 0));
+                else tc::commit_to(&mma_done);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---- drain: promote each segment into round-to-nearest FP32 sums; then C ----
+        const int quarter = warp & 3, half = (warp - 2) >> 2;
+        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+        const uint32_t tempty_leader = PAIR ? tc::mapa_shared(smem_u32(&tempty[0]), 0) : 0u;
+        uint8_t *stage = smem + L::EPI_OFFSET + (warp - 2) * kEpiTileBytes;
+        const int nseg = (p.kblocks + p.seg_kblocks - 1) / p.seg_kblocks;
+        const bool vec_ok = (p.ldc % 4 == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0) && (p.stride_c % 4 == 0);
+        int seg = -1;
+        bool ok = true;
+        for (int64_t t = unit; t < total && ok; t += units) {
+            int tm, tn, z;
+            decode(t, tm, tn, z);
+            const int64_t m0 = (int64_t)tm * L::TM + (int64_t)rank * 128;
+            const int64_t n0 = (int64_t)tn * BN;
+            float acc[BN / 2];
+#pragma unroll
+            for (int j = 0; j < BN / 2; ++j) acc[j] = 0.0f;
+            for (int g = 0; g < nseg; ++g) {
+                ++seg;
+                const int b = seg & 1;
+                if (!wait(&tfull[b], (uint32_t)(seg >> 1) & 1u, 2 * kWaitNs)) {
+                    if (!abort_flag) report_fault(p.fault, kFaultTcEpilogueWait);
+                    abort_flag = 1;
+                    ok = false;
+                    break;
+                }
+                tc::fence_after_sync();
+                // 16-column loads keep the drain within the 168-register cap
+#pragma unroll
+                for (int c = 0; c < BN / 2 / 16; ++c) {
+                    uint32_t r[16];
+                    tc::tmem_ld_32x32b_x16(tmem + lane_base + (uint32_t)(b * BN + half * (BN / 2) + c * 16), r);
+                    tc::tmem_ld_wait();
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) acc[c * 16 + j] = __fadd_rn(acc[c * 16 + j], __uint_as_float(r[j]));
+                }
+                tc::fence_before_sync();
+                __syncwarp();
+                if (lane == 0) {
+                    if (!PAIR || leader) mbar_arrive(&tempty[b]);
+                    else tc::mbar_arrive_remote(tempty_leader + (uint32_t)(b * sizeof(uint64_t)));
+                }
+            }
+            if (!ok || abort_flag) break;
+            const int64_t row0 = m0 + quarter * 32;
+            const int64_t col0 = n0 + half * (BN / 2);
+            if (p.tma_store) {
+                // 32 x 32 chunks: row `lane` into the staging tile (128-byte
+                // swizzle: 16-byte chunk j of row r at (j ^ (r & 7))), then one
+                // TMA store; C = alpha * acc when gemm (beta is 0 on this path)
+#pragma unroll
+                for (int c = 0; c < BN / 2 / 32; ++c) {
+                    if (lane == 0) bulk_wait_read<0>();  // the previous store has read the staging tile
+                    __syncwarp();
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        float v[4];
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) {
+                            const float a = acc[c * 32 + j * 4 + e];
+                            v[e] = p.gemm ? __fmaf_rn(p.alpha, a, 0.0f) : a;
+                        }
+                        *reinterpret_cast<float4 *>(stage + lane * 128 + ((j ^ (lane & 7)) << 4)) =
+                            make_float4(v[0], v[1], v[2], v[3]);
+                    }
+                    fence_proxy_async_shared();
+                    __syncwarp();
+                    if (lane == 0 && row0 < p.M && col0 + c * 32 < p.N) {
+                        tma_store_3d(&tcout, stage, (int32_t)(col0 + c * 32), (int32_t)row0, z);
+                        bulk_commit();
+                    }
+                }
+            } else {
+                const int64_t row = row0 + lane;
+                float *crow = p.C + (int64_t)z * p.stride_c + row * p.ldc;
+                if (row < p.M) {
+#pragma unroll
+                    for (int j = 0; j < BN / 2; j += 4) {
+                        float v[4];
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) {
+                            const int64_t col = col0 + j + e;
+                            if (p.gemm) {
+                                const float bc = (p.beta == 0.0f || col >= p.N) ? 0.0f : p.beta * crow[col];
+                                v[e] = __fmaf_rn(p.alpha, acc[j + e], bc);
+                            } else {
+                                v[e] = acc[j + e];
+                            }
+                        }
+                        if (vec_ok && col0 + j + 3 < p.N) {
+                            *reinterpret_cast<float4 *>(crow + col0 + j) = make_float4(v[0], v[1], v[2], v[3]);
+                        } else {
+#pragma unroll
+                            for (int e = 0; e < 4; ++e)
+                                if (col0 + j + e < p.N) crow[col0 + j + e] = v[e];
+                        }
+                    }
+                }
+            }
+        }
+        if (lane == 0) bulk_wait<0>();  // this warp's C stores are complete
+        __syncwarp();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (threadIdx.x == 0 && abort_flag) {
+        // Copies complete on the leader's barrier and cannot be awaited from
+        // a pair's second CTA: give every copy in flight time to land (they
+        // take microseconds).  The MMA issuer's CTA also waits for the MMAs
+        // issued before its abort.
+        const uint64_t t0 = tc::globaltimer();
+        while (tc::globaltimer() - t0 < 20000000ull) {
+        }
+        if (leader && mma_aborted) tc::wait_timed(&mma_done, 0, kWaitNs, nullptr);
+    }
+    __syncthreads();
+    if constexpr (PAIR) {
+        tc::cluster_sync();  // neither CTA leaves while the pair can still touch its memory
+        if (warp == 0) tc::tmem_dealloc_pair(tmem, kTmemCols2);
+    } else {
+        if (warp == 0) tc::tmem_dealloc(tmem, kTmemCols2);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // split pass: FP32 -> NP BF16 pieces, K-major [batch][rows][Kp]
 // ---------------------------------------------------------------------------
 struct SplitArgs {
@@ -966,6 +1300,68 @@ static WsPtrs ws_ptrs(const Plan &pl, void *ws) {
 // TFLOP/s; BF16 and FP8 run faster as single CTAs), 2 = always, 0 = never.
 static int g_tc_pair = 1;
 
+// Persistent launch: as many CTAs (CTA pairs) as fit on the GPU at once, at
+// most one per tile.  C leaves through a TMA tensor map unless beta is used
+// or C is not 16-byte aligned in rows and instances.
+template <int MODE, bool PAIR>
+static int launch_persistent(const CUtensorMap *ta, const CUtensorMap *tb, const Geometry &g, Params p,
+                             cudaStream_t stream) {
+    using PL = PersistentLayout<MODE, PAIR>;
+    auto kern = tc_gemm_persistent_kernel<MODE, PAIR>;
+    const int smem = (int)PL::SMEM_BYTES;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "tc persistent smem attribute: %s", cudaGetErrorString(e));
+    const int64_t tiles_m = (g.M + PL::TM - 1) / PL::TM, tiles_n = (g.N + BN - 1) / BN;
+    const int64_t total = tiles_m * tiles_n * g.batch;
+    if (tiles_m * tiles_n > 0x7fffffff || total > ((int64_t)1 << 40))
+        return set_error(GATLAS_ERR_INVALID, "matmul: too many tensor-core tiles");
+    p.tiles_m = (int)tiles_m;
+    p.tiles_n = (int)tiles_n;
+    p.batch = (int)g.batch;
+    CUtensorMap tcout = ta[0];  // unused unless tma_store
+    p.tma_store = 0;
+    const bool c_ok = (!p.gemm || p.beta == 0.0f) && aligned_to(p.C, 16) && p.ldc % 4 == 0 &&
+                      (g.batch == 1 || p.stride_c % 4 == 0) && g.N < ((int64_t)1 << 31) && g.M < ((int64_t)1 << 31);
+    if (c_ok) {
+        const uint64_t cdims[3] = {(uint64_t)g.N, (uint64_t)g.M, (uint64_t)g.batch};
+        const uint64_t cstr[2] = {(uint64_t)p.ldc * 4, (uint64_t)(g.batch > 1 ? p.stride_c : g.M * p.ldc) * 4};
+        const uint32_t cbox[3] = {32, 32, 1};
+        if (make_tensor_map(&tcout, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, p.C, cdims, cstr, cbox,
+                            CU_TENSOR_MAP_SWIZZLE_128B) == GATLAS_OK)
+            p.tma_store = 1;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.blockDim = dim3(kThreads2, 1, 1);
+    cfg.dynamicSmemBytes = (size_t)smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = PAIR ? 2 : 1;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = PAIR ? 1 : 0;
+    // resident units: CTAs (one per SM) or clusters of two, as the occupancy query reports
+    static thread_local int cap_dev = -1, cap = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cap_dev != dev) {
+        cap = PAIR ? sm_count() / 2 : sm_count();
+        if (PAIR) {
+            cfg.gridDim = dim3(2 * (unsigned)cap, 1, 1);
+            int n = 0;
+            if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) == cudaSuccess && n > 0) cap = n;
+            cudaGetLastError();
+        }
+        cap_dev = dev;
+    }
+    const int units = (int)std::min<int64_t>(total, std::max(cap, 1));
+    cfg.gridDim = dim3((unsigned)((PAIR ? 2 : 1) * units), 1, 1);
+    e = cudaLaunchKernelEx(&cfg, kern, ta[0], ta[1], ta[2], tb[0], tb[1], tb[2], tcout, p);
+    if (e != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "tc_gemm_persistent_kernel: %s", cudaGetErrorString(e));
+    return check_launch("tc_gemm_persistent_kernel");
+}
+
 template <int MODE>
 static int launch_tc(const Geometry &g, const Plan &pl, const WsPtrs &w, float *C, double alpha, double beta,
                      int gemm, int seg_kblocks, cudaStream_t stream) {
@@ -1009,6 +1405,10 @@ static int launch_tc(const Geometry &g, const Plan &pl, const WsPtrs &w, float *
     if (MODE == 3 && p.kblocks != pl.kblocks) return set_error(GATLAS_ERR_INVALID, "matmul: FP8 slice count");
     if (MODE == 3 && p.kblocks > kMaxFp8Blocks)
         return set_error(GATLAS_ERR_UNSUPPORTED, "matmul: FP8 engine takes K <= %d", kMaxFp8Blocks * 128);
+    if constexpr (MODE != 3) {
+        return pair ? launch_persistent<MODE, true>(ta, tb, g, p, stream)
+                    : launch_persistent<MODE, false>(ta, tb, g, p, stream);
+    } else {
     if (pair) {
         using PL = PairLayout<MODE>;
         const int smem = (int)PL::SMEM_BYTES;
@@ -1041,6 +1441,7 @@ static int launch_tc(const Geometry &g, const Plan &pl, const WsPtrs &w, float *
     dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)g.batch);
     tc_gemm_kernel<MODE><<<grid, kThreads2, smem, stream>>>(ta[0], ta[1], ta[2], tb[0], tb[1], tb[2], p);
     return check_launch("tc_gemm_kernel");
+    }
 }
 
 static int check_ws(const Plan &pl, const void *ws, size_t ws_bytes) {

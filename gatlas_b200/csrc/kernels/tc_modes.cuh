@@ -118,6 +118,35 @@ struct PairLayout {
     static_assert(STAGES >= 3, "pair pipeline depth");
 };
 
+// Persistent layout (BF16 modes): the ring, then one 32 x 32 FP32 staging
+// tile per drain warp for the TMA-store epilogue, which runs while the ring
+// already feeds the next tile.  PAIR: a 256 x 256 tile per cluster of two
+// CTAs, each staging its 128 rows of A and its 128-row half of B.
+constexpr uint32_t kEpiTileBytes = 32 * 32 * 4;
+constexpr uint32_t kEpiBytes = 8 * kEpiTileBytes;
+template <int MODE, bool PAIR, uint32_t ROWB = Mode<MODE>::ROWB>
+struct PersistentLayout {
+    using MD = Mode<MODE>;
+    static constexpr int NP = MD::NP;
+    static constexpr uint32_t ROW_BYTES = ROWB;
+    static constexpr int BK = (int)(ROWB / MD::ELEM);
+    static constexpr uint32_t SWIZZLE = ROWB == 128 ? tc::kSwizzle128B : tc::kSwizzle64B;
+    static constexpr uint32_t SBO = 8 * ROWB;
+    static constexpr int KSTEPS = (int)(ROWB / 32);
+    static constexpr int TM = PAIR ? 256 : 128;                    // rows of C per tile
+    static constexpr uint32_t A_TILE = 128 * ROWB;                 // this CTA's rows of A
+    static constexpr uint32_t B_TILE = (PAIR ? 128u : 256u) * ROWB;  // B's 256 rows, or this CTA's half
+    static constexpr uint32_t STAGE_BYTES = NP * (A_TILE + B_TILE);
+    static constexpr uint32_t BUDGET = 226 * 1024;
+    static constexpr int FIT = (int)((BUDGET - kEpiBytes - 1024) / STAGE_BYTES);
+    static constexpr int STAGES = FIT < 8 ? FIT : 8;
+    static constexpr uint32_t EPI_OFFSET = STAGES * STAGE_BYTES;
+    static constexpr uint32_t SMEM_BYTES = EPI_OFFSET + kEpiBytes + 1024;  // + alignment slack
+    static constexpr uint32_t IDESC = tc::idesc_bf16_f32(TM, 256);
+    static_assert(!MD::SCALED, "persistent layout: BF16 modes");
+    static_assert(STAGES >= 2, "tensor-core pipeline depth");
+};
+
 template <int NP>
 __device__ __forceinline__ void split_value(float x, __nv_bfloat16 (&out)[3]) {
     const __nv_bfloat16 hi = __float2bfloat16_rn(x);
