@@ -39,7 +39,10 @@
 namespace gatlas {
 namespace tcg {
 
-constexpr int kGroupM = 16;  // tile rows per raster group
+constexpr int kGroupM = 16;  // tile rows per raster group (128-row tiles)
+// Rows of C per raster group: 2048, i.e. 16 single-CTA or 8 pair tiles, so
+// that the tiles in flight at once (one per SM) cover a near-square block of
+// C whose A rows and B columns stay in L2.
 constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s bound on any single wait
 
 struct Params {
@@ -59,6 +62,7 @@ struct Params {
     // when C leaves through the C tensor map (beta == 0, 16-byte aligned)
     int tiles_m, tiles_n, batch;
     int tma_store;
+    int group_tiles;  // tile rows per raster group
 };
 
 // Warp roles: warp 0 = TMA producer (lane 0), warp 1 = MMA issuer (lane 0),
@@ -698,9 +702,10 @@ __global__ void __launch_bounds__(kThreads2, 1)
     auto decode = [&](int64_t t, int &tm, int &tn, int &z) {
         z = (int)(t / per_batch);
         const int bid = (int)(t - (int64_t)z * per_batch);
-        const int per_group = kGroupM * p.tiles_n;
-        const int first_m = (bid / per_group) * kGroupM;
-        const int gm = min(p.tiles_m - first_m, kGroupM);
+        const int G = p.group_tiles;
+        const int per_group = G * p.tiles_n;
+        const int first_m = (bid / per_group) * G;
+        const int gm = min(p.tiles_m - first_m, G);
         const int r = bid % per_group;
         tm = first_m + r % gm;
         tn = r / gm;
@@ -1299,6 +1304,8 @@ static WsPtrs ws_ptrs(const Plan &pl, void *ws) {
 // B200 (the split engines: at 8192^3 split3 491 vs 476 and split6 257 vs 242
 // TFLOP/s; BF16 and FP8 run faster as single CTAs), 2 = always, 0 = never.
 static int g_tc_pair = 1;
+// Rows of C per raster group of the persistent kernels (multiple of 128).
+static int g_tc_group_rows = kGroupM * 128;
 
 // Persistent launch: as many CTAs (CTA pairs) as fit on the GPU at once, at
 // most one per tile.  C leaves through a TMA tensor map unless beta is used
@@ -1318,6 +1325,7 @@ static int launch_persistent(const CUtensorMap *ta, const CUtensorMap *tb, const
     p.tiles_m = (int)tiles_m;
     p.tiles_n = (int)tiles_n;
     p.batch = (int)g.batch;
+    p.group_tiles = std::max(1, g_tc_group_rows / PL::TM);
     CUtensorMap tcout = ta[0];  // unused unless tma_store
     p.tma_store = 0;
     const bool c_ok = (!p.gemm || p.beta == 0.0f) && aligned_to(p.C, 16) && p.ldc % 4 == 0 &&
@@ -1661,6 +1669,12 @@ extern "C" int gatlas_set_option(const char *name, int64_t value) {
         tcg::g_tc_pair = (int)value;
         return GATLAS_OK;
     }
+    if (std::strcmp(name, "tc_group_rows") == 0) {
+        if (value < 128 || value > 65536 || value % 128 != 0)
+            return set_error(GATLAS_ERR_INVALID, "set_option: tc_group_rows is a multiple of 128 in [128, 65536]");
+        tcg::g_tc_group_rows = (int)value;
+        return GATLAS_OK;
+    }
     return set_error(GATLAS_ERR_INVALID, "set_option: unknown option %s", name);
 }
 
@@ -1669,6 +1683,10 @@ extern "C" int gatlas_get_option(const char *name, int64_t *value) {
     if (!name || !value) return set_error(GATLAS_ERR_INVALID, "get_option: null argument");
     if (std::strcmp(name, "tc_pair") == 0) {
         *value = tcg::g_tc_pair;
+        return GATLAS_OK;
+    }
+    if (std::strcmp(name, "tc_group_rows") == 0) {
+        *value = tcg::g_tc_group_rows;
         return GATLAS_OK;
     }
     return set_error(GATLAS_ERR_INVALID, "get_option: unknown option %s", name);

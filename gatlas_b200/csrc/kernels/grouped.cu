@@ -7,9 +7,9 @@
 // kernel per problem.  Design for B200:
 //  1. pack pass (one launch for all instances): every FP32 operand is split
 //     into BF16 pieces and written tile-major in the exact shared-memory
-//     image the MMA descriptors read: A as [mt][kt][128 rows x 64 B], B as
-//     [nt][kt][BN rows x 64 B], each tile 64-byte swizzled (16-byte chunk c
-//     of row r stored at chunk c ^ ((r >> 1) & 3)), zero padded past M, N, K.
+//     image the MMA descriptors read: A as [mt][kt][128 rows x 128 B], B as
+//     [nt][kt][BN rows x 128 B], each tile 128-byte swizzled (16-byte chunk
+//     c of row r stored at chunk c ^ (r & 7)), zero padded past M, N, K.
 //     The contraction then streams every tile with one 1-D bulk copy: no
 //     per-instance tensor maps;
 //  2. contraction: one CTA per SM walks a statically balanced list of
@@ -42,16 +42,16 @@ namespace gatlas {
 namespace grp {
 
 using tcg::BM;
-constexpr int kBK = 32;                  // BF16 elements per K slice
-constexpr uint32_t kRowBytes = 64;        // one K slice of one row
+constexpr int kBK = 64;                  // BF16 elements per K slice
+constexpr uint32_t kRowBytes = 128;       // one K slice of one row
 constexpr uint32_t kATileBytes = BM * kRowBytes;
 constexpr int kDrainWarps = 8;
 constexpr int kThreads = 32 * (2 + kDrainWarps);
 constexpr uint32_t kTmemCols = 512;       // two accumulators of up to 256 columns
 constexpr uint64_t kWaitNs = 2000000000ull;
 constexpr int kPackRows = 128;            // rows per pack item
-// The grouped engine stages 64-byte K slices (its packed tiles carry the
-// 64-byte swizzle) and promotes after the same K as the single-instance
+// The grouped engine stages 128-byte K slices (its packed tiles carry the
+// 128-byte swizzle) and promotes after the same K as the single-instance
 // engine (512 for one-product BF16, 256 for split3), issuing the same MMA
 // sequence, so that each instance's result is bit-identical to it.
 template <int MODE>
@@ -61,7 +61,7 @@ constexpr int grouped_seg_kblocks(int mode) { return (mode == 0 ? 512 : 256) / k
 // Packed byte offset of 16-byte chunk c of row `row` in K slice kb.
 __device__ __forceinline__ int64_t packed_offset(int64_t row, int kb, int c, int tr, int kt) {
     return ((row / tr) * kt + kb) * (int64_t)tr * kRowBytes + (row % tr) * kRowBytes +
-           ((c ^ (int)((row >> 1) & 3)) << 4);
+           ((c ^ (int)(row & 7)) << 4);
 }
 
 // ---------------------------------------------------------------------------
@@ -100,15 +100,16 @@ __device__ __forceinline__ PackItem pack_item(const Inst *insts, const int64_t *
     return q;
 }
 
-// The 16 values thread `tid` contributes to an item's 128 x 32 tile: four
+// The 32 values thread `tid` contributes to an item's 128 x 64 tile: eight
 // groups of 4 consecutive elements of the stored inner dimension.
-__device__ __forceinline__ void pack_load(const PackItem &q, int tid, float (&x)[16]) {
+constexpr int kPackGroups = kPackRows * kBK / 4 / 256;
+__device__ __forceinline__ void pack_load(const PackItem &q, int tid, float (&x)[4 * kPackGroups]) {
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < kPackGroups; ++i) {
         const int e = i * 256 + tid;
         int64_t outer, inner, outer_lim, inner_lim;
-        if (!q.transposed) {  // element (r, k) at src[r*ld + k]: 8 threads x 4 consecutive k per row
-            outer = q.r0 + (e >> 3), inner = q.k0 + (e & 7) * 4, outer_lim = q.rows, inner_lim = q.K;
+        if (!q.transposed) {  // element (r, k) at src[r*ld + k]: 16 threads x 4 consecutive k per row
+            outer = q.r0 + (e >> 4), inner = q.k0 + (e & 15) * 4, outer_lim = q.rows, inner_lim = q.K;
         } else {              // element (r, k) at src[k*ld + r]: 32 threads x 4 consecutive rows per k
             outer = q.k0 + (e >> 5), inner = q.r0 + (e & 31) * 4, outer_lim = q.K, inner_lim = q.rows;
         }
@@ -134,7 +135,7 @@ __device__ __forceinline__ void pack_load(const PackItem &q, int tid, float (&x)
 // an incremental walk, and neighbouring items read neighbouring memory.  The
 // next item's loads are in flight while the current one is split and stored.
 template <int NP>
-__global__ void __launch_bounds__(256, 4) grouped_pack_kernel(const Inst *insts, const int64_t *seg_start, int nseg,
+__global__ void __launch_bounds__(256, 2) grouped_pack_kernel(const Inst *insts, const int64_t *seg_start, int nseg,
                                                            int64_t per_cta) {
     __shared__ float tile[kPackRows][kBK + 1];
     const int tid = threadIdx.x;
@@ -154,16 +155,16 @@ __global__ void __launch_bounds__(256, 4) grouped_pack_kernel(const Inst *insts,
     }
     while (it0 >= seg_start[sgi + 1]) ++sgi;
     PackItem cur = pack_item(insts, seg_start, sgi, it0);
-    float x[16];
+    float x[4 * kPackGroups];
     pack_load(cur, tid, x);
     for (int64_t it = it0; it < it1; ++it) {
         __syncthreads();  // the previous item's reads of the tile are done
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < kPackGroups; ++i) {
             const int e = i * 256 + tid;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                if (!cur.transposed) tile[e >> 3][(e & 7) * 4 + j] = x[i * 4 + j];
+                if (!cur.transposed) tile[e >> 4][(e & 15) * 4 + j] = x[i * 4 + j];
                 else tile[(e & 31) * 4 + j][e >> 5] = x[i * 4 + j];
             }
         }
@@ -176,8 +177,8 @@ __global__ void __launch_bounds__(256, 4) grouped_pack_kernel(const Inst *insts,
             pack_load(next, tid, x);
         }
         uint8_t *const *dst = cur.op ? cur.I->pb : cur.I->pa;
-        for (int e = tid; e < kPackRows * 4; e += 256) {
-            const int r = e >> 2, c = e & 3;
+        for (int e = tid; e < kPackRows * (kBK / 8); e += 256) {
+            const int r = e >> 3, c = e & 7;
             const int64_t row = cur.r0 + r;
             if (row >= cur.rows_alloc) continue;
             __nv_bfloat16 pcs[8][3];
@@ -216,7 +217,7 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
     using L = GLayout<MODE>;
     using MD = tcg::Mode<MODE>;
     constexpr int S = L::STAGES;
-    static_assert(L::BK == kBK, "grouped engine stages BF16 slices of 32");
+    static_assert(L::BK == kBK, "grouped engine stages BF16 slices of 64");
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     __shared__ __align__(8) uint64_t full[S], empty[S], tfull[2], tempty[2], mma_done;

@@ -27,8 +27,9 @@ def _packed_bytes(m, n, k, bn, np_):
     r = lambda x: (x + 1023) // 1024 * 1024
     if m == 0 or n == 0:
         return 0
-    mt, nt, kt = -(-m // 128), -(-n // bn), -(-k // 32)
-    return np_ * (r(mt * kt * 128 * 64) + r(nt * kt * bn * 64))
+    # tiles of 128-byte K slices (64 BF16 elements) per row
+    mt, nt, kt = -(-m // 128), -(-n // bn), -(-k // 64)
+    return np_ * (r(mt * kt * 128 * 128) + r(nt * kt * bn * 128))
 
 
 @pytest.mark.parametrize("engine,np_", [("tc_bf16", 1), ("tc_split3", 2)])
