@@ -1003,55 +1003,91 @@ struct SplitArgs {
     int64_t piece_stride;                 // elements per instance in each piece: rows*Kp
 };
 
+// Stores the NP pieces of 8 consecutive elements of one K-major row: one
+// 16-byte store per piece (Kp is a multiple of 8, so every run is aligned).
 template <int NP>
-__global__ void __launch_bounds__(256) split_direct_kernel(SplitArgs a) {
-    const int64_t quads_per_row = a.Kp / 4;
-    const int64_t total = a.rows * quads_per_row;
-    const int64_t z = blockIdx.y;
-    const float *src = a.src + z * a.src_stride;
-    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t r = q / quads_per_row, k = (q % quads_per_row) * 4;
-        __nv_bfloat16 pcs[4][3];
+__device__ __forceinline__ void store_pieces8(const SplitArgs &a, int64_t z, int64_t r, int64_t k, const float (&x)[8]) {
+    __nv_bfloat16 pcs[8][3];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const float x = (k + e < a.K) ? src[r * a.ld + k + e] : 0.0f;
-            split_value<NP>(x, pcs[e]);
-        }
+    for (int e = 0; e < 8; ++e) split_value<NP>(x[e], pcs[e]);
 #pragma unroll
-        for (int i = 0; i < NP; ++i) {
-            __nv_bfloat162 v0 = __halves2bfloat162(pcs[0][i], pcs[1][i]);
-            __nv_bfloat162 v1 = __halves2bfloat162(pcs[2][i], pcs[3][i]);
-            uint2 u;
-            u.x = *reinterpret_cast<uint32_t *>(&v0);
-            u.y = *reinterpret_cast<uint32_t *>(&v1);
-            *reinterpret_cast<uint2 *>(a.out[i] + z * a.piece_stride + r * a.Kp + k) = u;
+    for (int i = 0; i < NP; ++i) {
+        uint32_t w[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            __nv_bfloat162 v = __halves2bfloat162(pcs[2 * j][i], pcs[2 * j + 1][i]);
+            w[j] = *reinterpret_cast<uint32_t *>(&v);
         }
+        *reinterpret_cast<uint4 *>(a.out[i] + z * a.piece_stride + r * a.Kp + k) = make_uint4(w[0], w[1], w[2], w[3]);
     }
 }
 
-// Source stored K x rows (element (r,k) at src[k*ld + r]); 32 x 32 tiles
-// transposed through shared memory so both the reads and the writes coalesce.
+// Source stored rows x K (element (r,k) at src[r*ld + k]): each thread
+// splits runs of 8 consecutive k, read as two 16-byte loads where aligned.
+template <int NP>
+__global__ void __launch_bounds__(256) split_direct_kernel(SplitArgs a) {
+    const int64_t runs_per_row = a.Kp / 8;
+    const int64_t total = a.rows * runs_per_row;
+    const int64_t z = blockIdx.y;
+    const float *src = a.src + z * a.src_stride;
+    const bool vec = (a.ld % 4 == 0) && ((reinterpret_cast<uintptr_t>(src) & 15) == 0);
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = q / runs_per_row, k = (q % runs_per_row) * 8;
+        const float *ptr = src + r * a.ld + k;
+        float x[8];
+        if (vec && k + 7 < a.K) {
+            const float4 u = __ldcs(reinterpret_cast<const float4 *>(ptr));
+            const float4 v = __ldcs(reinterpret_cast<const float4 *>(ptr + 4));
+            x[0] = u.x, x[1] = u.y, x[2] = u.z, x[3] = u.w, x[4] = v.x, x[5] = v.y, x[6] = v.z, x[7] = v.w;
+        } else {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) x[e] = (k + e < a.K) ? ptr[e] : 0.0f;
+        }
+        store_pieces8<NP>(a, z, r, k, x);
+    }
+}
+
+// Source stored K x rows (element (r,k) at src[k*ld + r]): 64 x 64 tiles
+// transposed through shared memory.  Reads are 16-byte loads along rows;
+// writes are 16-byte runs of 8 k, eight threads covering one 128-byte row
+// segment per piece.
 template <int NP>
 __global__ void __launch_bounds__(256) split_transpose_kernel(SplitArgs a) {
-    __shared__ float tile[32][33];
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
-    const int64_t r0 = (int64_t)blockIdx.x * 32, k0 = (int64_t)blockIdx.y * 32;
+    __shared__ float tile[64][65];  // [k][r]
+    const int tid = threadIdx.x;
+    const int64_t r0 = (int64_t)blockIdx.x * 64, k0 = (int64_t)blockIdx.y * 64;
     const int64_t z = blockIdx.z;
     const float *src = a.src + z * a.src_stride;
+    const bool vec = (a.ld % 4 == 0) && ((reinterpret_cast<uintptr_t>(src) & 15) == 0);
 #pragma unroll
-    for (int j = 0; j < 32; j += 8) {
-        const int64_t k = k0 + ty + j, r = r0 + tx;
-        tile[ty + j][tx] = (k < a.K && r < a.rows) ? src[k * a.ld + r] : 0.0f;
+    for (int p = 0; p < 4; ++p) {
+        const int kk = p * 16 + (tid >> 4), rr = (tid & 15) * 4;
+        const int64_t k = k0 + kk, r = r0 + rr;
+        float v[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        if (k < a.K) {
+            const float *ptr = src + k * a.ld + r;
+            if (vec && r + 3 < a.rows) {
+                const float4 u = __ldcs(reinterpret_cast<const float4 *>(ptr));
+                v[0] = u.x, v[1] = u.y, v[2] = u.z, v[3] = u.w;
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                    if (r + e < a.rows) v[e] = ptr[e];
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e) tile[kk][rr + e] = v[e];
     }
     __syncthreads();
 #pragma unroll
-    for (int j = 0; j < 32; j += 8) {
-        const int64_t r = r0 + ty + j, k = k0 + tx;
+    for (int p = 0; p < 2; ++p) {
+        const int rr = p * 32 + (tid >> 3), c = tid & 7;
+        const int64_t r = r0 + rr, k = k0 + c * 8;
         if (r < a.rows && k < a.Kp) {
-            __nv_bfloat16 pcs[3];
-            split_value<NP>(tile[tx][ty + j], pcs);
+            float x[8];
 #pragma unroll
-            for (int i = 0; i < NP; ++i) a.out[i][z * a.piece_stride + r * a.Kp + k] = pcs[i];
+            for (int j = 0; j < 8; ++j) x[j] = tile[c * 8 + j][rr];
+            store_pieces8<NP>(a, z, r, k, x);
         }
     }
 }
@@ -1258,7 +1294,7 @@ static int launch_split(int np, bool transposed, const float *src, int64_t rows,
     for (int i = 0; i < 3; ++i) a.out[i] = out[i];
     a.piece_stride = rows * Kp;
     if (!transposed) {
-        const int64_t total = rows * (Kp / 4);
+        const int64_t total = rows * (Kp / 8);
         int64_t grid = (total + 255) / 256;
         const int64_t cap = (int64_t)sm_count() * 16;
         if (grid > cap) grid = cap;
@@ -1267,7 +1303,7 @@ static int launch_split(int np, bool transposed, const float *src, int64_t rows,
         else if (np == 2) split_direct_kernel<2><<<gr, 256, 0, stream>>>(a);
         else split_direct_kernel<3><<<gr, 256, 0, stream>>>(a);
     } else {
-        const int64_t gx = (rows + 31) / 32, gy = (Kp + 31) / 32;
+        const int64_t gx = (rows + 63) / 64, gy = (Kp + 63) / 64;
         if (gy > 65535) return set_error(GATLAS_ERR_INVALID, "matmul: K too large for the transposing split");
         dim3 gr((unsigned)gx, (unsigned)gy, (unsigned)batch);
         if (np == 1) split_transpose_kernel<1><<<gr, 256, 0, stream>>>(a);
