@@ -54,9 +54,11 @@ def _peaks():
                 "source": "fallback"}
 
 
-# DRAM bytes (read + write) per launch of the split3 contraction at 8192^3,
-# from an ncu capture of the full-size launch (profiles/tc_gemm_kernel_split3_8192.md)
-TC_TRAFFIC_BYTES = 2.28e9 + 0.2555e9
+# DRAM bytes (read + write) per launch of the split3 contraction at 8192^3
+# (persistent kernel on CTA pairs), from an ncu capture of the full-size
+# launch (profiles/tc_gemm_persistent_split3_pair_8192.md)
+TC_TRAFFIC_BYTES = 3.181e9 + 0.264e9
+TC_KERNEL = "tc_gemm_persistent_kernel<split3, CTA pair>"
 
 # nominal FP32 SIMT peak: 148 SMs x 128 FP32 lanes x 2 flop x 1.965 GHz
 FP32_SIMT_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
@@ -488,14 +490,14 @@ def run_ours(args, rank, world, local):
         run_ms = _timed(lambda: g.matmul_tc_run(ws, M, N, K, C, engine=engine), args.steps, 2,
                         world, stream)
         ach = PRODUCTS[engine] * flops / (run_ms * 1e-3) / 1e12
-        roofline = {"bound": "tensor", "kernel": "tc_gemm_kernel<split3>", "achieved": ach,
+        roofline = {"bound": "tensor", "kernel": TC_KERNEL, "achieved": ach,
                     "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
                     "frac": ach / peaks["bf16_tflops"], "traffic": TC_TRAFFIC_BYTES,
                     "kernel_ms": run_ms, "kernel_fp32_equiv_tflops": flops / (run_ms * 1e-3) / 1e12,
                     "peak_source": f"{peaks['source']} dense BF16 (burst, cuBLAS); achieved counts all "
                                    f"{PRODUCTS[engine]} BF16 products per FP32 multiply-add; 'of measured'",
                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
-                                      "profiles/tc_gemm_kernel_split3_8192.md"}
+                                      "profiles/tc_gemm_persistent_split3_pair_8192.md"}
     else:
         roofline = {"bound": "fp32_simt", "achieved": value, "peak": FP32_SIMT_NOMINAL_TFLOPS,
                     "unit": "TFLOP/s", "frac": value / FP32_SIMT_NOMINAL_TFLOPS, "traffic": None,
@@ -761,6 +763,64 @@ def run_case(spec: str) -> None:
     print(json.dumps({"case": spec, "faults": g.device_faults()}))
 
 
+def run_tc_sweep(args) -> None:
+    """Sustained timing of the tensor-core contraction on prepared operands:
+    per size, engine, CTA-pair setting (0 single, 2 pairs) and raster group
+    height, about `--sweep-seconds` of back-to-back launches with the SM clock
+    sampled through NVML.  One JSON line per point; cycles = ms x median MHz."""
+    import time
+
+    import torch
+
+    import gatlas_b200 as g
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    engines = args.sweep_engines.split(",")
+    rows_list = [int(x) for x in args.sweep_group_rows.split(",")]
+    for M in (int(x) for x in args.tc_sweep.split(",")):
+        A = torch.empty(M * M, device=dev)
+        B = torch.empty(M * M, device=dev)
+        C = torch.empty(M * M, device=dev)
+        g.fill(A, "uniform", seed=1)
+        g.fill(B, "uniform", seed=2)
+        for eng in engines:
+            for pair in (0, 2):
+                g.set_option("tc_pair", pair)
+                ws = torch.empty(g.matmul_workspace_size(M, M, M, eng) + 1024, dtype=torch.uint8, device=dev)
+                ws = ws[(-ws.data_ptr()) % 1024:]
+                g.matmul_tc_prepare(A, B, M, M, M, ws, engine=eng)
+                for rows in rows_list:
+                    g.set_option("tc_group_rows", rows)
+                    for _ in range(3):
+                        g.matmul_tc_run(ws, M, M, M, C, engine=eng)
+                    torch.cuda.synchronize()
+                    t0 = time.perf_counter()
+                    g.matmul_tc_run(ws, M, M, M, C, engine=eng)
+                    torch.cuda.synchronize()
+                    n = max(10, int(args.sweep_seconds / max(time.perf_counter() - t0, 1e-6)))
+                    sampler = ClockSampler(0)
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    sampler.start()
+                    e0.record()
+                    for _ in range(n):
+                        g.matmul_tc_run(ws, M, M, M, C, engine=eng)
+                    e1.record()
+                    torch.cuda.synchronize()
+                    clocks = sampler.stop()
+                    ms = e0.elapsed_time(e1) / n
+                    mhz = clocks.get("sm_mhz")
+                    work = PRODUCTS.get(eng, 1) * 2.0 * M ** 3
+                    print(json.dumps({"m": M, "engine": eng, "pair": pair, "group_rows": rows, "launches": n,
+                                      "ms": round(ms, 4), "tflops_fp32_work": round(2.0 * M ** 3 / ms / 1e9, 1),
+                                      "tflops_tensor_work": round(work / ms / 1e9, 1), "sm_mhz": mhz,
+                                      "mcycles": round(ms * mhz / 1e3, 3) if mhz else None,
+                                      "reasons": clocks.get("reasons"), "faults": g.device_faults()}), flush=True)
+                del ws
+                torch.cuda.empty_cache()
+    g.set_option("tc_pair", 1)
+    g.set_option("tc_group_rows", 2048)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -772,7 +832,16 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--quick", action="store_true", help="skip the precision sweep")
     ap.add_argument("--case", default=None, help="run one small single-kernel case (for ncu) and exit")
+    ap.add_argument("--tc-sweep", default=None,
+                    help="sizes (comma-separated): sustained timing of the tensor-core contraction on single CTAs "
+                         "and CTA pairs, with SM clocks, one JSON line per point, then exit")
+    ap.add_argument("--sweep-engines", default="tc_bf16,tc_split3,tc_split6")
+    ap.add_argument("--sweep-group-rows", default="2048", help="raster group heights to sweep (multiples of 128)")
+    ap.add_argument("--sweep-seconds", type=float, default=1.5)
     args = ap.parse_args()
+    if args.tc_sweep:
+        run_tc_sweep(args)
+        return
     if args.case:
         run_case(args.case)
         return
