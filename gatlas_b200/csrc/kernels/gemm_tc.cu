@@ -11,15 +11,19 @@
 //     three pieces hi + mid + lo represent x exactly) written K-major
 //     ([rows][Kp], Kp = K rounded up to 8, zero padded), transposing the
 //     operands whose stored layout is not K-major;
-//  2. contraction: one CTA per 128 x 256 tile of C, 128 threads.  Warp 0
-//     lane 0 streams BK = 32 slices of every piece of A and B with 3-D TMA
-//     tensor-map loads (64-byte swizzle) into a multi-stage mbarrier ring;
-//     warp 1 lane 0 issues tcgen05.mma kind::f16 (M=128, N=256, K=16) for
-//     each product of pieces (hi·hi, hi·lo, lo·hi for 3 products; the six
-//     leading products of three pieces for 6), accumulating in FP32 in TMEM
-//     (256 columns); after the last slice all four warps read the
-//     accumulator back with tcgen05.ld 32x32b and apply
-//     C = fma(alpha, acc, beta*C).
+//  2. contraction (BF16, split3, split6): a persistent kernel, one CTA per
+//     SM over 128 x 256 tiles of C, or one cluster of two CTAs per SM pair
+//     over 256 x 256 tiles (cta_group::2).  Warp 0 lane 0 streams K slices
+//     of 128 bytes per row (64 BF16; 64 bytes for split6) of every piece
+//     of A and B with 3-D TMA tensor-map loads (128-byte swizzle) into a
+//     multi-stage mbarrier ring; warp 1 lane 0 issues tcgen05.mma kind::f16
+//     (M = 128 or 256, N = 256, K = 16) for each product of pieces (hi*hi,
+//     hi*lo, lo*hi for 3 products; the six leading products of three pieces
+//     for 6), accumulating in FP32 in two TMEM buffers of 256 columns; eight
+//     drain warps promote each segment into round-to-nearest FP32 registers
+//     and, at the end of a tile, apply C = fma(alpha, acc, beta*C) and store
+//     C through TMA while the next tile already runs.  FP8 E4M3 (per-block
+//     scales) runs one tile per CTA (tc_gemm_kernel / tc_gemm_pair_kernel).
 // Every mbarrier wait is bounded in wall time; a timeout sets the device
 // fault word, stops the pipeline, drains the copies in flight and frees TMEM.
 #include <cuda.h>

@@ -192,7 +192,9 @@ int gatlas_matmul_f32_host(const gatlas_matmul_desc *d, const float *A, const fl
  * CTA staging half of B) or one CTA per 128 x 256 tile: 1 (default) where
  * pairs measure faster (the split3 and split6 engines), 2 always, 0 never.  Results
  * are bit-identical either way (same pieces, same MMA order, same
- * promotion). */
+ * promotion).  "tc_group_rows": rows of C per raster group of the
+ * persistent tensor-core contraction, a multiple of 128 (default 2048): the
+ * tiles in flight cover a block of that height, whose operands share L2. */
 int gatlas_set_option(const char *name, int64_t value);
 int gatlas_get_option(const char *name, int64_t *value);
 
