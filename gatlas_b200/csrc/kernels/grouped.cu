@@ -11,7 +11,8 @@
 //     [nt][kt][BN rows x 128 B], each tile 128-byte swizzled (16-byte chunk
 //     c of row r stored at chunk c ^ (r & 7)), zero padded past M, N, K.
 //     The contraction then streams every tile with one 1-D bulk copy: no
-//     per-instance tensor maps;
+//     per-instance tensor maps.  The pack itself stages its source tiles
+//     with 16-byte async copies through a 3-stage shared-memory ring;
 //  2. contraction: one CTA per SM walks a statically balanced list of
 //     output tiles (longest first, greedy onto the least-loaded CTA) across
 //     instances.  Warp 0 streams tiles through the mbarrier ring, warp 1
@@ -100,44 +101,66 @@ __device__ __forceinline__ PackItem pack_item(const Inst *insts, const int64_t *
     return q;
 }
 
-// The 32 values thread `tid` contributes to an item's 128 x 64 tile: eight
-// groups of 4 consecutive elements of the stored inner dimension.
-constexpr int kPackGroups = kPackRows * kBK / 4 / 256;
-__device__ __forceinline__ void pack_load(const PackItem &q, int tid, float (&x)[4 * kPackGroups]) {
+// Stage layout: [128 rows][64 k] floats (rows of 256 B) for row-major
+// sources, [64 k][128 rows] (k rows of 512 B) for transposed ones, where the
+// 16-byte chunk of rows 4q..4q+3 in k row k sits at chunk q ^ ((k >> 3) & 7),
+// so that the eight k-runs one warp reads per row land in distinct banks.
+constexpr uint32_t kPackTileBytes = kPackRows * kBK * 4;
+constexpr int kPackStages = 3;
+constexpr uint32_t kPackSmemBytes = kPackStages * kPackTileBytes;
+constexpr int kPackChunks = (int)(kPackTileBytes / 16) / 256;  // 16-byte chunks per thread per item
+
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(smem_dst)), "l"(src),
+                 "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem_dst, const void *src, uint32_t src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_u32(smem_dst)), "l"(src),
+                 "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Thread `tid` copies its 16-byte chunks of item q into `stage` with async
+// copies (no registers held while they fly); bytes past M, N or K are
+// zero-filled by the copies themselves.
+__device__ __forceinline__ void pack_issue(const PackItem &q, uint8_t *stage, int tid) {
 #pragma unroll
-    for (int i = 0; i < kPackGroups; ++i) {
-        const int e = i * 256 + tid;
+    for (int j = 0; j < kPackChunks; ++j) {
+        const int e = j * 256 + tid;
         int64_t outer, inner, outer_lim, inner_lim;
-        if (!q.transposed) {  // element (r, k) at src[r*ld + k]: 16 threads x 4 consecutive k per row
+        if (!q.transposed) {  // stage[r][k]: 16 chunks per 256-byte row
             outer = q.r0 + (e >> 4), inner = q.k0 + (e & 15) * 4, outer_lim = q.rows, inner_lim = q.K;
-        } else {              // element (r, k) at src[k*ld + r]: 32 threads x 4 consecutive rows per k
+        } else {              // stage[k][r]: 32 chunks per 512-byte k row
             outer = q.k0 + (e >> 5), inner = q.r0 + (e & 31) * 4, outer_lim = q.K, inner_lim = q.rows;
         }
+        int64_t valid = outer < outer_lim ? inner_lim - inner : 0;
+        valid = valid < 0 ? 0 : (valid > 4 ? 4 : valid);
+        const float *src = valid > 0 ? q.src + outer * q.ld + inner : q.src;
+        uint8_t *dst = !q.transposed ? stage + (size_t)e * 16
+                                     : stage + (size_t)(e >> 5) * 512 + (((e & 31) ^ ((e >> 8) & 7)) << 4);
+        if (q.vec) {
+            cp_async16(dst, src, (uint32_t)valid * 4);
+        } else {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) x[i * 4 + j] = 0.0f;
-        if (outer < outer_lim) {
-            const float *ptr = q.src + outer * q.ld + inner;
-            if (q.vec && inner + 3 < inner_lim) {
-                const float4 v = __ldcs(reinterpret_cast<const float4 *>(ptr));
-                x[i * 4] = v.x, x[i * 4 + 1] = v.y, x[i * 4 + 2] = v.z, x[i * 4 + 3] = v.w;
-            } else {
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    if (inner + j < inner_lim) x[i * 4 + j] = ptr[j];
-            }
+            for (int v = 0; v < 4; ++v) cp_async4(dst + 4 * v, v < valid ? src + v : q.src, v < valid ? 4u : 0u);
         }
     }
 }
 
-// Item space: segment s = 2*instance + operand covers rows/128 x kt items,
-// ordered row block major, K slice minor.  CTA b packs the contiguous items
-// [b*per_cta, (b+1)*per_cta): one binary search for its first segment, then
-// an incremental walk, and neighbouring items read neighbouring memory.  The
-// next item's loads are in flight while the current one is split and stored.
+// One walk per CTA over its items: every thread keeps kPackStages - 1 items
+// of async copies in flight while the CTA splits the current item from
+// shared memory into BF16 pieces and writes them with 16-byte swizzled
+// stores.
 template <int NP>
 __global__ void __launch_bounds__(256, 2) grouped_pack_kernel(const Inst *insts, const int64_t *seg_start, int nseg,
                                                            int64_t per_cta) {
-    __shared__ float tile[kPackRows][kBK + 1];
+    extern __shared__ __align__(128) uint8_t pack_smem[];
     const int tid = threadIdx.x;
     const int64_t nitems = seg_start[nseg];
     const int64_t it0 = (int64_t)blockIdx.x * per_cta;
@@ -154,52 +177,70 @@ __global__ void __launch_bounds__(256, 2) grouped_pack_kernel(const Inst *insts,
         sgi = lo;
     }
     while (it0 >= seg_start[sgi + 1]) ++sgi;
-    PackItem cur = pack_item(insts, seg_start, sgi, it0);
-    float x[4 * kPackGroups];
-    pack_load(cur, tid, x);
+    auto stage_of = [&](int64_t it) { return pack_smem + (size_t)((it - it0) % kPackStages) * kPackTileBytes; };
+
+    // issue cursor: one commit group per item (empty past the range), so that
+    // wait_group counts items
+    int psgi = sgi;
+    int64_t pit = it0;
+    auto issue_next = [&]() {
+        if (pit < it1) {
+            while (pit >= seg_start[psgi + 1]) ++psgi;
+            pack_issue(pack_item(insts, seg_start, psgi, pit), stage_of(pit), tid);
+        }
+        cp_async_commit();
+        ++pit;
+    };
+    for (int i = 0; i < kPackStages - 1; ++i) issue_next();
+
     for (int64_t it = it0; it < it1; ++it) {
-        __syncthreads();  // the previous item's reads of the tile are done
-#pragma unroll
-        for (int i = 0; i < kPackGroups; ++i) {
-            const int e = i * 256 + tid;
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                if (!cur.transposed) tile[e >> 4][(e & 15) * 4 + j] = x[i * 4 + j];
-                else tile[(e & 31) * 4 + j][e >> 5] = x[i * 4 + j];
-            }
-        }
-        __syncthreads();
-        // next item: its loads fly while this one is split and stored
-        PackItem next = cur;
-        if (it + 1 < it1) {
-            while (it + 1 >= seg_start[sgi + 1]) ++sgi;
-            next = pack_item(insts, seg_start, sgi, it + 1);
-            pack_load(next, tid, x);
-        }
+        issue_next();  // into the stage the previous iteration released
+        cp_async_wait<kPackStages - 1>();  // this thread's copies of item `it` have landed
+        __syncthreads();                   // and every other thread's
+        while (it >= seg_start[sgi + 1]) ++sgi;
+        const PackItem cur = pack_item(insts, seg_start, sgi, it);
+        const float *tile = reinterpret_cast<const float *>(stage_of(it));
         uint8_t *const *dst = cur.op ? cur.I->pb : cur.I->pa;
-        for (int e = tid; e < kPackRows * (kBK / 8); e += 256) {
+#pragma unroll
+        for (int pass = 0; pass < kPackRows * (kBK / 8) / 256; ++pass) {
+            const int e = pass * 256 + tid;
+            // 8 threads per row (coalesced 128-byte runs of pieces), 4 rows per warp
             const int r = e >> 3, c = e & 7;
             const int64_t row = cur.r0 + r;
             if (row >= cur.rows_alloc) continue;
+            float x[8];
+            if (!cur.transposed) {
+                // the upper four threads read their second half first: no bank conflicts
+                const int h = (c >> 2) & 1;
+                const float4 u = *reinterpret_cast<const float4 *>(tile + r * kBK + c * 8 + 4 * h);
+                const float4 v = *reinterpret_cast<const float4 *>(tile + r * kBK + c * 8 + 4 * (h ^ 1));
+                const float4 lo = h ? v : u, hi = h ? u : v;
+                x[0] = lo.x, x[1] = lo.y, x[2] = lo.z, x[3] = lo.w, x[4] = hi.x, x[5] = hi.y, x[6] = hi.z, x[7] = hi.w;
+            } else {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int k = c * 8 + j;  // (k >> 3) & 7 == c
+                    x[j] = tile[k * kPackRows + ((((r >> 2) ^ c) << 2) | (r & 3))];
+                }
+            }
             __nv_bfloat16 pcs[8][3];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) tcg::split_value<NP>(tile[r][c * 8 + j], pcs[j]);
+            for (int j = 0; j < 8; ++j) tcg::split_value<NP>(x[j], pcs[j]);
             const int64_t off = packed_offset(row, cur.kb, c, cur.tr, cur.I->kt);
 #pragma unroll
             for (int i = 0; i < NP; ++i) {
-                uint4 u;
                 uint32_t w[4];
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     __nv_bfloat162 v = __halves2bfloat162(pcs[2 * j][i], pcs[2 * j + 1][i]);
                     w[j] = *reinterpret_cast<uint32_t *>(&v);
                 }
-                u.x = w[0], u.y = w[1], u.z = w[2], u.w = w[3];
-                *reinterpret_cast<uint4 *>(dst[i] + off) = u;
+                *reinterpret_cast<uint4 *>(dst[i] + off) = make_uint4(w[0], w[1], w[2], w[3]);
             }
         }
-        cur = next;
+        __syncthreads();  // this stage is read: the next issue may refill it
     }
+    cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------
@@ -622,14 +663,32 @@ int grouped_build(int engine, const gatlas_grouped_instance *in, int32_t count, 
     return GATLAS_OK;
 }
 
+// Shared-memory attribute of the pack kernels, once per device (also before
+// a graph capture, since attribute changes are not captured).
+static void grouped_pack_attributes() {
+    static thread_local int attr_dev = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (attr_dev == dev) return;
+    cudaFuncSetAttribute(grp::grouped_pack_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)grp::kPackSmemBytes);
+    cudaFuncSetAttribute(grp::grouped_pack_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)grp::kPackSmemBytes);
+    attr_dev = dev;
+}
+
 int grouped_launch_pack(const GroupedTables &t, const GroupedDevice &d, cudaStream_t stream) {
     if (t.nitems == 0) return GATLAS_OK;
-    const int64_t grid = std::min<int64_t>(t.nitems, (int64_t)sm_count() * 8);
+    // two resident CTAs per SM (96 KiB of staging each), one item range per CTA
+    grouped_pack_attributes();
+    const int64_t grid = std::min<int64_t>(t.nitems, (int64_t)sm_count() * 2);
     const int64_t per_cta = (t.nitems + grid - 1) / grid;
     if (t.np == 2)
-        grp::grouped_pack_kernel<2><<<(unsigned)grid, 256, 0, stream>>>(d.inst, d.seg, t.nseg, per_cta);
+        grp::grouped_pack_kernel<2><<<(unsigned)grid, 256, grp::kPackSmemBytes, stream>>>(d.inst, d.seg, t.nseg,
+                                                                                          per_cta);
     else
-        grp::grouped_pack_kernel<1><<<(unsigned)grid, 256, 0, stream>>>(d.inst, d.seg, t.nseg, per_cta);
+        grp::grouped_pack_kernel<1><<<(unsigned)grid, 256, grp::kPackSmemBytes, stream>>>(d.inst, d.seg, t.nseg,
+                                                                                          per_cta);
     return check_launch("grouped_pack_kernel");
 }
 
@@ -801,6 +860,7 @@ int grouped_launch_graph(GroupedPlan *p, int with_prepare, cudaStream_t stream) 
                              (int)grp::GLayout<0>::SMEM_BYTES);
         cudaFuncSetAttribute(grp::grouped_gemm_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)grp::GLayout<1>::SMEM_BYTES);
+        grouped_pack_attributes();
         device_fault_word();
         cudaGraph_t graph = nullptr;
         int rc = GATLAS_OK;

@@ -137,22 +137,45 @@ def test_promotion_interval_is_selectable(cuda):
 @pytest.mark.parametrize("engine", ENGINES + ["tc_fp8"])
 @pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
 @pytest.mark.parametrize("M,N,K", [(520, 300, 384), (256, 256, 4096), (129, 1000, 40)])
-def test_cta_pairs_match_single_ctas(cuda, engine, ta, tb, M, N, K):
+@pytest.mark.parametrize("beta", [0.5, 0.0])
+def test_cta_pairs_match_single_ctas(cuda, engine, ta, tb, M, N, K, beta):
     # 256 x 256 tiles on CTA pairs (cta_group::2) and 128 x 256 tiles on single
-    # CTAs run the same pieces through the same MMA order and promotion
+    # CTAs run the same pieces through the same MMA order and promotion; beta = 0
+    # stores C through TMA where C's rows are 16-byte aligned, beta != 0 reads it
     A = oracle.uniform(M * K, seed=M + K + ta)
     B = oracle.uniform(K * N, seed=N + K + tb)
     assert g.get_option("tc_pair") == 1
     try:
         g.set_option("tc_pair", 0)
         single = _mm(cuda, A, B, M, N, K, engine, ta, tb, gemm=True, Cin=oracle.uniform(M * N, seed=3),
-                     alpha=1.5, beta=0.5)
+                     alpha=1.5, beta=beta)
         g.set_option("tc_pair", 2)
         pair = _mm(cuda, A, B, M, N, K, engine, ta, tb, gemm=True, Cin=oracle.uniform(M * N, seed=3),
-                   alpha=1.5, beta=0.5)
+                   alpha=1.5, beta=beta)
     finally:
         g.set_option("tc_pair", 1)
     assert np.array_equal(single, pair)
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("rows", [128, 384, 65536])
+def test_raster_group_height_does_not_change_results(cuda, engine, rows):
+    # the persistent kernels visit tiles in groups of `rows` rows of C; every tile
+    # is computed the same way whatever the order (batched, ragged edges, both
+    # store paths: N = 700 keeps C's rows 16-byte aligned, N = 701 does not)
+    M, K, P = 1100, 300, 2
+    for N in (700, 701):
+        A = oracle.uniform(P * M * K, seed=21)
+        B = oracle.uniform(P * K * N, seed=22)
+        base = _mm(cuda, A, B, M, N, K, engine, batch=P)
+        g.set_option("tc_group_rows", rows)
+        try:
+            got = _mm(cuda, A, B, M, N, K, engine, batch=P)
+        finally:
+            g.set_option("tc_group_rows", 2048)
+        assert np.array_equal(base, got)
+        ref = oracle.matmul(A, B, M, N, K, mode=oracle.F64, packed=P)
+        assert oracle.normwise_error(got, ref) <= BUDGET[engine]
 
 
 @pytest.mark.parametrize("engine", ENGINES + ["tc_fp8", "buffer"])

@@ -82,3 +82,12 @@ def test_options_round_trip_without_a_device():
         g.set_option("no_such_option", 1)
     with pytest.raises(g.GatlasError, match="0, 1 or 2"):
         g.set_option("tc_pair", 3)
+    assert g.get_option("tc_group_rows") == 2048
+    g.set_option("tc_group_rows", 384)
+    try:
+        assert g.get_option("tc_group_rows") == 384
+    finally:
+        g.set_option("tc_group_rows", 2048)
+    for bad in (0, 100, 129, 65536 + 128):
+        with pytest.raises(g.GatlasError, match="multiple of 128"):
+            g.set_option("tc_group_rows", bad)
