@@ -67,6 +67,14 @@ struct Params {
     int tiles_m, tiles_n, batch;
     int tma_store;
     int group_tiles;  // tile rows per raster group
+    // FP8 persistent kernel: per tile (instance-major, then tile row, then
+    // tile column) the segment count, one segment-start bit per 128-deep
+    // block (plan_words words), and each segment's scale products of the
+    // tile's two column halves (kblocks entries reserved per tile)
+    const int *plan_nseg;
+    const uint32_t *plan_bits;
+    const float2 *plan_q;
+    int plan_words;
 };
 
 // Warp roles: warp 0 = TMA producer (lane 0), warp 1 = MMA issuer (lane 0),
@@ -76,285 +84,13 @@ constexpr int kDrainWarps = 8;
 constexpr int kThreads2 = 32 * (2 + kDrainWarps);
 constexpr uint32_t kTmemCols2 = 2 * BN;  // two accumulator buffers
 
-template <int MODE>
-__global__ void __launch_bounds__(kThreads2, 1)
-    tc_gemm_kernel(const __grid_constant__ CUtensorMap ta0, const __grid_constant__ CUtensorMap ta1,
-                   const __grid_constant__ CUtensorMap ta2, const __grid_constant__ CUtensorMap tb0,
-                   const __grid_constant__ CUtensorMap tb1, const __grid_constant__ CUtensorMap tb2,
-                   Params p) {
-    using L = Layout<MODE>;
-    using MD = Mode<MODE>;
-    constexpr int S = L::STAGES;
-    extern __shared__ uint8_t smem_raw[];
-    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    __shared__ __align__(8) uint64_t full[S], empty[S], tfull[2], tempty[2];
-    __shared__ uint32_t tmem_base;
-    __shared__ volatile int abort_flag;
-    __shared__ int kb_issued, kb_consumed;
-
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // Grouped raster: consecutive CTAs walk kGroupM tile rows before moving to
-    // the next tile column, so that a wave of resident CTAs shares A and B
-    // tiles through L2 instead of re-reading all of B from DRAM every wave.
-    int tile_m, tile_n;
-    {
-        const int tiles_n = gridDim.x, tiles_m = gridDim.y;
-        const int bid = blockIdx.y * tiles_n + blockIdx.x;
-        const int per_group = kGroupM * tiles_n;
-        const int first_m = (bid / per_group) * kGroupM;
-        const int gm = min(tiles_m - first_m, kGroupM);
-        const int r = bid % per_group;
-        tile_m = first_m + r % gm;
-        tile_n = r / gm;
-    }
-    const int m0 = tile_m * BM, n0 = tile_n * BN, z = blockIdx.z;
-    constexpr int BK = L::BK;
-    const CUtensorMap *tA[3] = {&ta0, &ta1, &ta2};
-    const CUtensorMap *tB[3] = {&tb0, &tb1, &tb2};
-    __shared__ int fp8_nseg;
-
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < S; ++s) {
-            mbar_init(&full[s], 1);
-            mbar_init(&empty[s], 1);
-        }
-        for (int b = 0; b < 2; ++b) {
-            mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], kDrainWarps);
-        }
-        fence_mbarrier_init();
-        abort_flag = 0;
-        kb_issued = 0;
-        kb_consumed = 0;
-        for (int i = 0; i < MD::NP; ++i) {
-            prefetch_tmap(tA[i]);
-            prefetch_tmap(tB[i]);
-        }
-    }
-    if (warp == 0) {
-        tc::tmem_alloc(&tmem_base, kTmemCols2);
-        tc::tmem_relinquish();
-    }
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
-    const uint32_t tmem = tmem_base;
-
-    // Segment plan.  BF16 modes: fixed runs of seg_kblocks slices.  FP8: a
-    // segment is a run of at most seg_kblocks 128-deep blocks whose scale
-    // products sa*sb are equal for both column halves of the tile; the
-    // tensor core accumulates the run in TMEM and the drain scales it once,
-    // which is exact because the scales are powers of two.
-    float *seg_q0 = nullptr, *seg_q1 = nullptr;
-    uint8_t *seg_flag = nullptr;
-    int nseg = (p.kblocks + p.seg_kblocks - 1) / p.seg_kblocks;
-    if constexpr (MD::SCALED) {
-        seg_q0 = reinterpret_cast<float *>(smem + S * L::STAGE_BYTES);
-        seg_q1 = seg_q0 + kMaxFp8Blocks;
-        seg_flag = reinterpret_cast<uint8_t *>(seg_q1 + kMaxFp8Blocks);
-        const int nb0 = tile_n * 2;
-        const float *sa = p.scale_a + z * p.scale_a_stride + (int64_t)tile_m * p.kblocks;
-        const float *sb0 = nb0 < p.nblocks_n ? p.scale_b + z * p.scale_b_stride + (int64_t)nb0 * p.kblocks : nullptr;
-        const float *sb1 =
-            nb0 + 1 < p.nblocks_n ? p.scale_b + z * p.scale_b_stride + (int64_t)(nb0 + 1) * p.kblocks : nullptr;
-        for (int kb = threadIdx.x; kb < p.kblocks; kb += blockDim.x) {
-            const float a = sa[kb];
-            seg_q0[kb] = sb0 ? __fmul_rn(a, sb0[kb]) : 0.0f;
-            seg_q1[kb] = sb1 ? __fmul_rn(a, sb1[kb]) : 0.0f;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int s = -1, run = 0;
-            float prev0 = 0.0f, prev1 = 0.0f;
-            for (int kb = 0; kb < p.kblocks; ++kb) {
-                const float q0 = seg_q0[kb], q1 = seg_q1[kb];
-                const bool start = kb == 0 || run == p.seg_kblocks || q0 != prev0 || q1 != prev1;
-                if (start) {
-                    ++s;
-                    run = 0;
-                    seg_q0[s] = q0;  // s <= kb: compacted in place
-                    seg_q1[s] = q1;
-                }
-                seg_flag[kb] = start ? 1 : 0;
-                ++run;
-                prev0 = q0;
-                prev1 = q1;
-            }
-            fp8_nseg = s + 1;
-        }
-        __syncthreads();
-        nseg = fp8_nseg;
-    }
-
-    auto a_tile = [&](int s, int piece) { return smem + s * L::STAGE_BYTES + piece * L::A_TILE; };
-    auto b_tile = [&](int s, int piece) { return smem + s * L::STAGE_BYTES + MD::NP * L::A_TILE + piece * L::B_TILE; };
-
-    if (warp == 0) {
-        if (lane == 0) {
-            // ---- TMA producer ----
-            int kb = 0;
-            for (; kb < p.kblocks; ++kb) {
-                const int s = kb % S;
-                const uint32_t ph = (uint32_t)(kb / S) & 1u;
-                if (!tc::wait_timed(&empty[s], ph ^ 1u, kWaitNs, &abort_flag)) {
-                    if (!abort_flag) report_fault(p.fault, kFaultTcProducerWait);
-                    abort_flag = 1;
-                    break;
-                }
-                mbar_arrive_expect_tx(&full[s], L::STAGE_BYTES);
-                for (int i = 0; i < MD::NP; ++i) {
-                    tma_load_3d(a_tile(s, i), tA[i], kb * BK, m0, z, &full[s]);
-                    tma_load_3d(b_tile(s, i), tB[i], kb * BK, n0, z, &full[s]);
-                }
-            }
-            kb_issued = kb;
-        }
-        __syncwarp();
-    } else if (warp == 1) {
-        if (lane == 0) {
-            // ---- MMA issuer: segment g accumulates into TMEM buffer g & 1 ----
-            constexpr uint32_t idesc = L::IDESC;
-            int kb = 0, seg = -1;
-            for (; kb < p.kblocks; ++kb) {
-                bool seg_first, seg_last;
-                if constexpr (MD::SCALED) {
-                    seg_first = seg_flag[kb] != 0;
-                    seg_last = kb == p.kblocks - 1 || seg_flag[kb + 1] != 0;
-                } else {
-                    seg_first = (kb % p.seg_kblocks) == 0;
-                    seg_last = (kb % p.seg_kblocks) == p.seg_kblocks - 1 || kb == p.kblocks - 1;
-                }
-                if (seg_first) ++seg;
-                const int b = seg & 1;
-                if (seg_first) {
-                    // the drain of this buffer's previous segment must be done
-                    if (!tc::wait_timed(&tempty[b], ((uint32_t)(seg >> 1) & 1u) ^ 1u, kWaitNs, &abort_flag)) {
-                        if (!abort_flag) report_fault(p.fault, kFaultTcMmaWait);
-                        abort_flag = 1;
-                        break;
-                    }
-                    tc::fence_after_sync();
-                }
-                const int s = kb % S;
-                const uint32_t ph = (uint32_t)(kb / S) & 1u;
-                if (!tc::wait_timed(&full[s], ph, kWaitNs, &abort_flag)) {
-                    if (!abort_flag) report_fault(p.fault, kFaultTcMmaWait);
-                    abort_flag = 1;
-                    break;
-                }
-                tc::fence_after_sync();
-                const uint32_t d = tmem + (uint32_t)(b * BN);
-#pragma unroll
-                for (int kk = 0; kk < L::KSTEPS; ++kk) {
-#pragma unroll
-                    for (int j = 0; j < MD::NPROD; ++j) {
-                        // 32 bytes of K per instruction inside the swizzled rows
-                        const uint32_t a_addr = smem_u32(a_tile(s, MD::pa(j))) + kk * 32;
-                        const uint32_t b_addr = smem_u32(b_tile(s, MD::pb(j))) + kk * 32;
-                        const uint64_t ad = tc::smem_desc_kmajor(a_addr, L::SBO, L::SWIZZLE);
-                        const uint64_t bd = tc::smem_desc_kmajor(b_addr, L::SBO, L::SWIZZLE);
-                        const uint32_t accum = (seg_first && kk == 0 && j == 0) ? 0u : 1u;
-                        if constexpr (MD::SCALED) tc::mma_f8(d, ad, bd, idesc, accum);
-                        else tc::mma_bf16(d, ad, bd, idesc, accum);
-                    }
-                }
-                tc::commit_to(&empty[s]);
-                if (seg_last) tc::commit_to(&tfull[b]);
-            }
-            kb_consumed = kb;
-            if (kb < p.kblocks) {
-                // aborted: make sure every issued MMA has completed before TMEM is freed
-                tc::commit_to(&tfull[0]);
-            }
-        }
-        __syncwarp();
-    } else {
-        // ---- drain: promote each segment into round-to-nearest FP32 sums ----
-        const int quarter = warp & 3, half = (warp - 2) >> 2;
-        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
-        float acc[BN / 2];
-#pragma unroll
-        for (int j = 0; j < BN / 2; ++j) acc[j] = 0.0f;
-        bool ok = true;
-        for (int seg = 0; seg < nseg; ++seg) {
-            const int b = seg & 1;
-            float scale = 1.0f;
-            if constexpr (MD::SCALED) scale = half ? seg_q1[seg] : seg_q0[seg];  // this half's scale block
-            if (!tc::wait_timed(&tfull[b], (uint32_t)(seg >> 1) & 1u, 2 * kWaitNs, &abort_flag)) {
-                if (!abort_flag) report_fault(p.fault, kFaultTcEpilogueWait);
-                abort_flag = 1;
-                ok = false;
-                break;
-            }
-            tc::fence_after_sync();
-#pragma unroll
-            for (int c = 0; c < BN / 2 / 32; ++c) {
-                uint32_t r[32];
-                tc::tmem_ld_32x32b_x32(tmem + lane_base + (uint32_t)(b * BN + half * (BN / 2) + c * 32), r);
-                tc::tmem_ld_wait();
-#pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    if constexpr (MD::SCALED)
-                        acc[c * 32 + j] = __fmaf_rn(__uint_as_float(r[j]), scale, acc[c * 32 + j]);
-                    else
-                        acc[c * 32 + j] = __fadd_rn(acc[c * 32 + j], __uint_as_float(r[j]));
-                }
-            }
-            tc::fence_before_sync();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&tempty[b]);
-        }
-        if (ok && !abort_flag) {
-            const int64_t row = (int64_t)m0 + quarter * 32 + lane;
-            float *crow = p.C + (int64_t)z * p.stride_c + row * p.ldc;
-            const bool vec_ok = (p.ldc % 4 == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0) &&
-                                (p.stride_c % 4 == 0);
-            if (row < p.M) {
-                const int64_t col0 = (int64_t)n0 + half * (BN / 2);
-#pragma unroll
-                for (int j = 0; j < BN / 2; j += 4) {
-                    float v[4];
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const int64_t col = col0 + j + e;
-                        if (p.gemm) {
-                            const float bc = (p.beta == 0.0f || col >= p.N) ? 0.0f : p.beta * crow[col];
-                            v[e] = __fmaf_rn(p.alpha, acc[j + e], bc);
-                        } else {
-                            v[e] = acc[j + e];
-                        }
-                    }
-                    if (vec_ok && col0 + j + 3 < p.N) {
-                        *reinterpret_cast<float4 *>(crow + col0 + j) = make_float4(v[0], v[1], v[2], v[3]);
-                    } else {
-#pragma unroll
-                        for (int e = 0; e < 4; ++e)
-                            if (col0 + j + e < p.N) crow[col0 + j + e] = v[e];
-                    }
-                }
-            }
-        }
-    }
-    tc::fence_before_sync();
-    __syncthreads();
-    if (threadIdx.x == 0 && abort_flag) {
-        // wait (bounded) for copies still landing in shared memory and for
-        // the MMAs issued before the abort
-        for (int kb = kb_consumed; kb < kb_issued; ++kb)
-            tc::wait_timed(&full[kb % S], (uint32_t)(kb / S) & 1u, kWaitNs, nullptr);
-        if (kb_consumed < p.kblocks) tc::wait_timed(&tfull[0], 0, kWaitNs, nullptr);
-    }
-    __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, kTmemCols2);
-}
-
 // ---------------------------------------------------------------------------
 // CTA-pair contraction (cta_group::2): one 256 x 256 tile per cluster of two
 // ---------------------------------------------------------------------------
 // Each CTA streams 128 rows of A and its 128-row half of B per K slice
 // (instead of 128 + 256 rows for a 128 x 256 tile), so the operand bytes
 // moved from L2 per FLOP fall by a third and the ring gets deeper for the
-// same shared memory.  Roles per CTA as in tc_gemm_kernel; only the leader
+// same shared memory.  Roles per CTA as in tc_gemm_persistent_kernel; only the leader
 // (rank 0) issues MMAs, M = 256 split by rows across the two TMEMs.
 // Barriers (no multicast forms anywhere):
 //  * full[s] of the leader: both producers' TMA loads complete on it; the
@@ -667,13 +403,17 @@ __global__ void __launch_bounds__(kThreads2, 1)
 }
 
 // ---------------------------------------------------------------------------
-// Persistent contraction (BF16 modes): one CTA (or CTA pair) per SM walks
+// Persistent contraction: one CTA (or CTA pair) per SM walks
 // the tiles t = unit, unit + units, ... in the grouped raster order.  The
 // ring, the MMA issue and the TMEM double buffer run on across tile
 // boundaries, so one tile's last promotions and its C stores overlap the
 // next tile's loads and MMAs; each drain warp stages its 32 x 128 block of C
 // through a 32 x 32 shared-memory tile (128-byte swizzle) and a TMA store,
 // which also clips the tile at M and N.  PAIR as in tc_gemm_pair_kernel.
+// FP8 (MODE 3, single CTAs): segments follow the per-tile plan written by
+// fp8_plan_kernel (runs of equally scaled 128-deep blocks); the MMA issuer
+// reads its segment-start bits a 32-block word ahead, the drain scales each
+// segment as it promotes it.
 // ---------------------------------------------------------------------------
 template <int MODE, bool PAIR>
 __global__ void __launch_bounds__(kThreads2, 1)
@@ -809,9 +549,29 @@ __global__ void __launch_bounds__(kThreads2, 1)
             uint32_t ph = 0;
             bool stop = false;
             for (int64_t t = unit; t < total && !stop; t += units) {
+                const uint32_t *wb = nullptr;
+                uint32_t wcur = 0, wnext = 0;
+                if constexpr (MD::SCALED) {
+                    int tm, tn, z;
+                    decode(t, tm, tn, z);
+                    wb = p.plan_bits + (((int64_t)z * p.tiles_m + tm) * p.tiles_n + tn) * p.plan_words;
+                    wcur = __ldg(wb);
+                    wnext = p.plan_words > 1 ? __ldg(wb + 1) : 0u;
+                }
                 for (int kb = 0; kb < p.kblocks; ++kb) {
-                    const bool seg_first = (kb % p.seg_kblocks) == 0;
-                    const bool seg_last = (kb % p.seg_kblocks) == p.seg_kblocks - 1 || kb == p.kblocks - 1;
+                    bool seg_first, seg_last;
+                    if constexpr (MD::SCALED) {
+                        if (kb > 0 && (kb & 31) == 0) {  // next word; the one after it loads meanwhile
+                            wcur = wnext;
+                            wnext = (kb >> 5) + 1 < p.plan_words ? __ldg(wb + (kb >> 5) + 1) : 0u;
+                        }
+                        const int k1 = kb + 1;
+                        seg_first = ((wcur >> (kb & 31)) & 1u) != 0;
+                        seg_last = k1 == p.kblocks || (((k1 & 31) ? (wcur >> (k1 & 31)) : wnext) & 1u) != 0;
+                    } else {
+                        seg_first = (kb % p.seg_kblocks) == 0;
+                        seg_last = (kb % p.seg_kblocks) == p.seg_kblocks - 1 || kb == p.kblocks - 1;
+                    }
                     if (seg_first) ++seg;
                     const int b = seg & 1;
                     if (seg_first) {
@@ -842,7 +602,8 @@ __global__ void __launch_bounds__(kThreads2, 1)
                             const uint64_t ad = tc::smem_desc_kmajor(a_addr, L::SBO, L::SWIZZLE);
                             const uint64_t bd = tc::smem_desc_kmajor(b_addr, L::SBO, L::SWIZZLE);
                             const uint32_t accum = (seg_first && kk == 0 && j == 0) ? 0u : 1u;
-                            if constexpr (PAIR) tc::mma_bf16_pair(d, ad, bd, idesc, accum);
+                            if constexpr (MD::SCALED) tc::mma_f8(d, ad, bd, idesc, accum);
+                            else if constexpr (PAIR) tc::mma_bf16_pair(d, ad, bd, idesc, accum);
                             else tc::mma_bf16(d, ad, bd, idesc, accum);
                         }
                     }
@@ -887,12 +648,24 @@ __global__ void __launch_bounds__(kThreads2, 1)
             decode(t, tm, tn, z);
             const int64_t m0 = (int64_t)tm * L::TM + (int64_t)rank * 128;
             const int64_t n0 = (int64_t)tn * BN;
+            int tile_nseg = nseg;
+            const float2 *tile_q = nullptr;
+            if constexpr (MD::SCALED) {
+                const int64_t pidx = ((int64_t)z * p.tiles_m + tm) * p.tiles_n + tn;
+                tile_nseg = __ldg(p.plan_nseg + pidx);
+                tile_q = p.plan_q + pidx * p.kblocks;
+            }
             float acc[BN / 2];
 #pragma unroll
             for (int j = 0; j < BN / 2; ++j) acc[j] = 0.0f;
-            for (int g = 0; g < nseg; ++g) {
+            for (int g = 0; g < tile_nseg; ++g) {
                 ++seg;
                 const int b = seg & 1;
+                float scale = 1.0f;
+                if constexpr (MD::SCALED) {
+                    const float2 q = __ldg(tile_q + g);  // this half's scale block product
+                    scale = half ? q.y : q.x;
+                }
                 if (!wait(&tfull[b], (uint32_t)(seg >> 1) & 1u, 2 * kWaitNs)) {
                     if (!abort_flag) report_fault(p.fault, kFaultTcEpilogueWait);
                     abort_flag = 1;
@@ -907,7 +680,12 @@ __global__ void __launch_bounds__(kThreads2, 1)
                     tc::tmem_ld_32x32b_x16(tmem + lane_base + (uint32_t)(b * BN + half * (BN / 2) + c * 16), r);
                     tc::tmem_ld_wait();
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) acc[c * 16 + j] = __fadd_rn(acc[c * 16 + j], __uint_as_float(r[j]));
+                    for (int j = 0; j < 16; ++j) {
+                        if constexpr (MD::SCALED)
+                            acc[c * 16 + j] = __fmaf_rn(__uint_as_float(r[j]), scale, acc[c * 16 + j]);
+                        else
+                            acc[c * 16 + j] = __fadd_rn(acc[c * 16 + j], __uint_as_float(r[j]));
+                    }
                 }
                 tc::fence_before_sync();
                 __syncwarp();
@@ -1229,9 +1007,10 @@ struct Plan {
     int elem;  // bytes per staged element
     int64_t Kp;
     size_t a_piece_bytes, b_piece_bytes;
-    // FP8: scale blocks
+    // FP8: scale blocks, and the per-tile segment plan of the contraction
     int64_t mblocks, nblocks, kblocks;
     size_t sa_bytes, sb_bytes;
+    size_t plan_nseg_bytes, plan_bits_bytes, plan_q_bytes;
     size_t total;
 };
 
@@ -1253,14 +1032,22 @@ static bool make_plan(const gatlas_matmul_desc *d, const Geometry &g, Plan *pl) 
     pl->b_piece_bytes = round_up((size_t)g.batch * (size_t)g.N * (size_t)pl->Kp * pl->elem, 1024);
     pl->mblocks = pl->nblocks = pl->kblocks = 0;
     pl->sa_bytes = pl->sb_bytes = 0;
+    pl->plan_nseg_bytes = pl->plan_bits_bytes = pl->plan_q_bytes = 0;
     if (pl->mode == 3) {
         pl->mblocks = (g.M + kQBlock - 1) / kQBlock;
         pl->nblocks = (g.N + kQBlock - 1) / kQBlock;
         pl->kblocks = (int64_t)((K + kQBlock - 1) / kQBlock);
         pl->sa_bytes = round_up((size_t)g.batch * pl->mblocks * pl->kblocks * 4, 1024);
         pl->sb_bytes = round_up((size_t)g.batch * pl->nblocks * pl->kblocks * 4, 1024);
+        // tiles of 128 x 256: per tile a segment count, one bit per block, a
+        // scale pair per possible segment
+        const size_t tiles = (size_t)((g.M + BM - 1) / BM) * (size_t)((g.N + BN - 1) / BN) * (size_t)g.batch;
+        pl->plan_nseg_bytes = round_up(tiles * 4, 256);
+        pl->plan_bits_bytes = round_up(tiles * (size_t)((pl->kblocks + 31) / 32) * 4, 256);
+        pl->plan_q_bytes = round_up(tiles * (size_t)pl->kblocks * 8, 1024);
     }
-    pl->total = pl->np * (pl->a_piece_bytes + pl->b_piece_bytes) + pl->sa_bytes + pl->sb_bytes;
+    pl->total = pl->np * (pl->a_piece_bytes + pl->b_piece_bytes) + pl->sa_bytes + pl->sb_bytes +
+                pl->plan_nseg_bytes + pl->plan_bits_bytes + pl->plan_q_bytes;
     return true;
 }
 
@@ -1322,6 +1109,9 @@ static int launch_split(int np, bool transposed, const float *src, int64_t rows,
 struct WsPtrs {
     void *a[3], *b[3];
     float *sa, *sb;
+    int *plan_nseg;  // FP8: per-tile segment plan (fp8_plan_kernel)
+    uint32_t *plan_bits;
+    float2 *plan_q;
 };
 
 static WsPtrs ws_ptrs(const Plan &pl, void *ws) {
@@ -1337,6 +1127,10 @@ static WsPtrs ws_ptrs(const Plan &pl, void *ws) {
     uint8_t *sc = base + pl.np * (pl.a_piece_bytes + pl.b_piece_bytes);
     w.sa = pl.mode == 3 ? reinterpret_cast<float *>(sc) : nullptr;
     w.sb = pl.mode == 3 ? reinterpret_cast<float *>(sc + pl.sa_bytes) : nullptr;
+    uint8_t *pp = sc + pl.sa_bytes + pl.sb_bytes;
+    w.plan_nseg = pl.mode == 3 ? reinterpret_cast<int *>(pp) : nullptr;
+    w.plan_bits = pl.mode == 3 ? reinterpret_cast<uint32_t *>(pp + pl.plan_nseg_bytes) : nullptr;
+    w.plan_q = pl.mode == 3 ? reinterpret_cast<float2 *>(pp + pl.plan_nseg_bytes + pl.plan_bits_bytes) : nullptr;
     return w;
 }
 
@@ -1346,6 +1140,52 @@ static WsPtrs ws_ptrs(const Plan &pl, void *ws) {
 static int g_tc_pair = 1;
 // Rows of C per raster group of the persistent kernels (multiple of 128).
 static int g_tc_group_rows = kGroupM * 128;
+
+// FP8 segment plan, one thread per 128 x 256 tile: a run of at most
+// seg_kblocks 128-deep blocks whose scale products sa * sb are equal for both
+// column halves of the tile accumulates in TMEM and is promoted, scaled once
+// (exact: the scales are powers of two).  Writes the tile's segment count,
+// its segment-start bits and each segment's two scale products.
+__global__ void __launch_bounds__(128)
+    fp8_plan_kernel(const float *scale_a, const float *scale_b, int64_t sa_stride, int64_t sb_stride, int tiles_m,
+                    int tiles_n, int batch, int kblocks, int nblocks_n, int seg_kblocks, int words, int *nseg,
+                    uint32_t *bits, float2 *q) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)tiles_m * tiles_n * batch) return;
+    const int tn = (int)(idx % tiles_n);
+    const int64_t rest = idx / tiles_n;
+    const int tm = (int)(rest % tiles_m);
+    const int64_t z = rest / tiles_m;
+    const float *sa = scale_a + z * sa_stride + (int64_t)tm * kblocks;
+    const int nb0 = 2 * tn, nb1 = 2 * tn + 1;
+    const float *sb0 = nb0 < nblocks_n ? scale_b + z * sb_stride + (int64_t)nb0 * kblocks : nullptr;
+    const float *sb1 = nb1 < nblocks_n ? scale_b + z * sb_stride + (int64_t)nb1 * kblocks : nullptr;
+    uint32_t *wb = bits + idx * words;
+    float2 *qt = q + idx * kblocks;
+    int s = -1, run = 0;
+    float prev0 = 0.0f, prev1 = 0.0f;
+    uint32_t w = 0;
+    for (int kb = 0; kb < kblocks; ++kb) {
+        const float a = sa[kb];
+        const float q0 = sb0 ? __fmul_rn(a, sb0[kb]) : 0.0f;
+        const float q1 = sb1 ? __fmul_rn(a, sb1[kb]) : 0.0f;
+        const bool start = kb == 0 || run == seg_kblocks || q0 != prev0 || q1 != prev1;
+        if (start) {
+            ++s;
+            run = 0;
+            qt[s] = make_float2(q0, q1);
+            w |= 1u << (kb & 31);
+        }
+        ++run;
+        prev0 = q0;
+        prev1 = q1;
+        if ((kb & 31) == 31 || kb == kblocks - 1) {
+            wb[kb >> 5] = w;
+            w = 0;
+        }
+    }
+    nseg[idx] = s + 1;
+}
 
 // Persistent launch: as many CTAs (CTA pairs) as fit on the GPU at once, at
 // most one per tile.  C leaves through a TMA tensor map unless beta is used
@@ -1433,6 +1273,7 @@ static int launch_tc(const Geometry &g, const Plan &pl, const WsPtrs &w, float *
         if (rc) return rc;
     }
     Params p;
+    std::memset(&p, 0, sizeof(p));
     p.C = C;
     p.M = g.M;
     p.N = g.N;
@@ -1481,14 +1322,22 @@ static int launch_tc(const Geometry &g, const Plan &pl, const WsPtrs &w, float *
         if (e != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "tc_gemm_pair_kernel: %s", cudaGetErrorString(e));
         return check_launch("tc_gemm_pair_kernel");
     }
-    const int smem = (int)L::SMEM_BYTES;
-    cudaError_t e = cudaFuncSetAttribute(tc_gemm_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "tc gemm smem attribute: %s", cudaGetErrorString(e));
-    const int64_t gx = (g.N + BN - 1) / BN, gy = (g.M + BM - 1) / BM;
-    if (gy > 65535) return set_error(GATLAS_ERR_INVALID, "matmul: M too large for the tensor-core grid");
-    dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)g.batch);
-    tc_gemm_kernel<MODE><<<grid, kThreads2, smem, stream>>>(ta[0], ta[1], ta[2], tb[0], tb[1], tb[2], p);
-    return check_launch("tc_gemm_kernel");
+    // single CTAs: plan every tile's segments, then the persistent kernel
+    const int64_t tiles_m = (g.M + BM - 1) / BM, tiles_n = (g.N + BN - 1) / BN;
+    const int64_t tiles = tiles_m * tiles_n * g.batch;
+    if (tiles > 0) {
+        const int words = (int)((p.kblocks + 31) / 32);
+        fp8_plan_kernel<<<(unsigned)((tiles + 127) / 128), 128, 0, stream>>>(
+            w.sa, w.sb, p.scale_a_stride, p.scale_b_stride, (int)tiles_m, (int)tiles_n, (int)g.batch, p.kblocks,
+            p.nblocks_n, p.seg_kblocks, words, w.plan_nseg, w.plan_bits, w.plan_q);
+        int rc = check_launch("fp8_plan_kernel");
+        if (rc) return rc;
+        p.plan_nseg = w.plan_nseg;
+        p.plan_bits = w.plan_bits;
+        p.plan_q = w.plan_q;
+        p.plan_words = words;
+    }
+    return launch_persistent<MODE, false>(ta, tb, g, p, stream);
     }
 }
 
@@ -1579,6 +1428,12 @@ static int run_rows(const gatlas_matmul_desc *d, const Plan &pl, const Geometry 
     for (int i = 0; i < 3; ++i)
         if (wb.a[i]) wb.a[i] = static_cast<uint8_t *>(wb.a[i]) + r0 * pl.Kp * pl.elem;
     if (wb.sa) wb.sa += (r0 / kQBlock) * pl.kblocks;
+    if (pl.mode == 3) {  // the block's tiles in the plan of the whole product
+        const int64_t first = (r0 / BM) * ((g.N + BN - 1) / BN);
+        wb.plan_nseg += first;
+        wb.plan_bits += first * ((pl.kblocks + 31) / 32);
+        wb.plan_q += first * pl.kblocks;
+    }
     float *Cb = C + r0 * g.ldc;
     switch (pl.mode) {
         case 0: return launch_tc<0>(gb, pb, wb, Cb, d->alpha, d->beta, d->gemm, (int)d->extra, s);

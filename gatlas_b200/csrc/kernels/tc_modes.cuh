@@ -120,7 +120,7 @@ struct PairLayout {
     static_assert(STAGES >= 3, "pair pipeline depth");
 };
 
-// Persistent layout (BF16 modes): the ring, then one 32 x 32 FP32 staging
+// Persistent layout: the ring, then one 32 x 32 FP32 staging
 // tile per drain warp for the TMA-store epilogue, which runs while the ring
 // already feeds the next tile.  PAIR: a 256 x 256 tile per cluster of two
 // CTAs, each staging its 128 rows of A and its 128-row half of B.
@@ -144,8 +144,8 @@ struct PersistentLayout {
     static constexpr int STAGES = FIT < 8 ? FIT : 8;
     static constexpr uint32_t EPI_OFFSET = STAGES * STAGE_BYTES;
     static constexpr uint32_t SMEM_BYTES = EPI_OFFSET + kEpiBytes + 1024;  // + alignment slack
-    static constexpr uint32_t IDESC = tc::idesc_bf16_f32(TM, 256);
-    static_assert(!MD::SCALED, "persistent layout: BF16 modes");
+    static constexpr uint32_t IDESC = MD::SCALED ? tc::idesc_e4m3_f32(TM, 256) : tc::idesc_bf16_f32(TM, 256);
+    static_assert(!(MD::SCALED && PAIR), "persistent FP8 runs on single CTAs");
     static_assert(STAGES >= 2, "tensor-core pipeline depth");
 };
 

@@ -142,9 +142,11 @@ int gatlas_matvec_f32_noalloc(const gatlas_matvec_desc *d, const float *A, const
  * amax / s <= 448); runs of up to `extra` (0 selects 4) 128-deep blocks
  * whose scale products sa * sb are equal accumulate in TMEM and are promoted
  * scaled once, exactly (powers of two), K <= 131072; its
- * tc_prepare workspace holds [A codes][B codes][A scales][B scales], codes
- * K-major [batch][rows][Kp] (Kp = K rounded up to 16), scales
- * [batch][rows/128][K/128], each part 1024-byte aligned. */
+ * tc_prepare workspace holds [A codes][B codes][A scales][B scales][plan],
+ * codes K-major [batch][rows][Kp] (Kp = K rounded up to 16), scales
+ * [batch][rows/128][K/128], each part 1024-byte aligned; tc_run writes the
+ * plan (each 128 x 256 tile's runs of equally scaled blocks) before it
+ * contracts. */
 typedef struct gatlas_matmul_desc {
     int32_t engine;
     int32_t gemm;
