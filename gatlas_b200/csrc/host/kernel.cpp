@@ -337,14 +337,18 @@ std::ostream &KernelMatmul::print(std::ostream &os) const {
        << " GEMM=" << generalizedMatmul() << " packed=" << packedCalc() << "\n";
     if (variant_ == Variant::TcFp8) {
         os << "// quant_fp8_kernel: E4M3 codes with one power-of-two FP32 scale per 128x128 block\n"
-           << "// tcgen05 kernel tc_gemm_kernel<tcfp8>: 128x256 output tile per CTA, TMA 128B-swizzled E4M3 tiles "
-           << "(BK=128), tcgen05.mma kind::f8f6f4 M=128 N=256 K=32, each 128-deep block scaled and promoted into "
-           << "FP32 registers\n";
+           << "// fp8_plan_kernel: per 128x256 tile, runs of up to " << (extraParam() ? extraParam() : 4)
+           << " equally scaled 128-deep blocks\n"
+           << "// tcgen05 kernel tc_gemm_persistent_kernel<tcfp8>: one CTA per SM over 128x256 output tiles, TMA "
+           << "128B-swizzled E4M3 tiles (BK=128), tcgen05.mma kind::f8f6f4 M=128 N=256 K=32, each run promoted "
+           << "scaled into FP32 registers, C stored through TMA\n";
     } else if (is_tc(variant_)) {
-        os << "// tcgen05 kernel tc_gemm_kernel<" << variant_name(variant_)
-           << ">: 128x256 output tile per CTA, TMA 64B-swizzled BF16 piece tiles (BK=32), "
-           << "tcgen05.mma kind::f16 M=128 N=256 K=16, FP32 accumulation in TMEM promoted every "
-           << (extraParam() ? extraParam() : (variant_ == Variant::TcBf16 ? 16 : 4)) << " K-slices\n";
+        const bool split6 = variant_ == Variant::TcSplit6, bf16 = variant_ == Variant::TcBf16;
+        os << "// tcgen05 kernel tc_gemm_persistent_kernel<" << variant_name(variant_)
+           << ">: one CTA per SM over 128x256 output tiles" << (bf16 ? "" : " (CTA pairs over 256x256 tiles when M > 128)")
+           << ", TMA " << (split6 ? "64B-swizzled BF16 piece tiles (BK=32)" : "128B-swizzled BF16 piece tiles (BK=64)")
+           << ", tcgen05.mma kind::f16 N=256 K=16, FP32 accumulation in TMEM promoted every "
+           << (extraParam() ? extraParam() : (bf16 ? 8 : 4)) << " K-slices, C stored through TMA\n";
     } else {
         const size_t bm = groupHeight() * blockHeight(), bn = groupWidth() * blockWidth();
         const bool img = variant_ == Variant::Image;

@@ -23,7 +23,9 @@
 //     drain warps promote each segment into round-to-nearest FP32 registers
 //     and, at the end of a tile, apply C = fma(alpha, acc, beta*C) and store
 //     C through TMA while the next tile already runs.  FP8 E4M3 (per-block
-//     scales) runs one tile per CTA (tc_gemm_kernel / tc_gemm_pair_kernel).
+//     scales) runs the same persistent kernel on single CTAs, its segments
+//     planned per tile by fp8_plan_kernel; FP8 pairs (opt-in) run one tile
+//     per cluster (tc_gemm_pair_kernel).
 // Every mbarrier wait is bounded in wall time; a timeout sets the device
 // fault word, stops the pipeline, drains the copies in flight and frees TMEM.
 #include <cuda.h>
