@@ -320,9 +320,19 @@ int ensure_slot(Slot &s, size_t bytes) {
     return GATLAS_OK;
 }
 
-int run_serial(Server &S, const gatlas_request *rq, int32_t count, gatlas_request_result *res) {
-    const int64_t t0 = now_ns();
+// Host and device timelines share their origin: the start event is recorded
+// and completed before the host clock starts, so a completion measured on the
+// device from the start event is never earlier, on the host's clock, than the
+// arrival it follows (latencies can only be overstated, by the microseconds
+// the synchronisation takes to return).
+int64_t start_clocks(Server &S) {
     cudaEventRecord(S.start, S.sg);
+    cudaEventSynchronize(S.start);
+    return now_ns();
+}
+
+int run_serial(Server &S, const gatlas_request *rq, int32_t count, gatlas_request_result *res) {
+    const int64_t t0 = start_clocks(S);
     cudaEvent_t ev = S.get_event();
     for (int i = 0; i < count; ++i) {
         const gatlas_request &r = rq[i];
@@ -360,8 +370,7 @@ int run_continuous(Server &S, const gatlas_request *rq, int32_t count, gatlas_re
     // work completes in launch order on each stream: harvest from the fronts
     std::deque<Flight> flights_g, flights_m;
     cudaEvent_t prep_ev = S.get_event();
-    const int64_t t0 = now_ns();
-    cudaEventRecord(S.start, S.sg);
+    const int64_t t0 = start_clocks(S);
     int next = 0, done = 0, gemm_inflight = 0;
     int blocked_head = -1;
     uint64_t blocked_epoch = 0;

@@ -130,6 +130,8 @@ def test_latency_accounting_on_a_poisson_trace(cuda):
         out = srv.run(req, mode)
         assert (out["status"] == 0).all()
         assert (out["admit_ns"] >= req["arrival_ns"]).all()
-        assert (out["done_ns"] >= out["admit_ns"] - 1000000).all()   # device clock vs host clock skew < 1 ms
+        # the device clock starts no later than the host clock: completions never
+        # precede their admission on the host's timeline
+        assert (out["done_ns"] >= out["admit_ns"]).all()
     with pytest.raises(g.GatlasError):
         srv.release({"result": 12345})
