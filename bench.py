@@ -520,7 +520,7 @@ def run_ours(args, rank, world, local):
            "h2d_bytes_per_step": 2 * M * K * 4, "d2h_bytes_per_step": M * N * 4,
            "ms_per_step": e2e_ms,
            "path": "gatlas_matmul_f32_host: pinned host A, B in, C out (B uploaded and split once, A in "
-                   "1024-row blocks whose uploads, splits, contraction and C downloads overlap)"}
+                   "512-row blocks whose uploads, splits, contraction and C downloads overlap on three streams)"}
     del hA, hB, hC
 
     # ---- precision sweep (8192^3; DGEMM 4096^3) -------------------------------

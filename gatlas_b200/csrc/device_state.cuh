@@ -30,7 +30,7 @@ constexpr int kScratchSlots = 2;
 void *device_scratch(size_t bytes, int slot = 0);
 
 // Per-device non-blocking streams owned by the library (created on first use).
-constexpr int kPoolStreams = 2;
+constexpr int kPoolStreams = 3;
 cudaStream_t pool_stream(int i);
 
 #ifdef __CUDACC__

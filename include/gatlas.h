@@ -183,10 +183,11 @@ int gatlas_matmul_tc_run(const gatlas_matmul_desc *d, const void *workspace, siz
  * returns before the work completes; synchronise the stream before reading
  * C).  Replaces the reference's bus-transfer timing modes -s/-r
  * (GatlasBenchmark.cpp:198-265).  Tensor-core engines with one instance and
- * M >= 2048 pipeline the transfers: B is uploaded and prepared once, then A
- * streams in blocks of 1024 rows whose uploads, preparation, contraction and
- * C downloads overlap on two library streams.  Use pinned host memory for
- * the copies to overlap.  Results are bit-identical to gatlas_matmul_f32. */
+ * M >= 1024 pipeline the transfers on three library streams: uploads (B,
+ * then A in blocks of 512 rows, back to back), preparation and contraction
+ * of each block as it lands, and the download of each block's C rows as
+ * its contraction finishes.  Use pinned host memory for the copies to
+ * overlap.  Results are bit-identical to gatlas_matmul_f32. */
 int gatlas_matmul_f32_host(const gatlas_matmul_desc *d, const float *A, const float *B, float *C, void *stream);
 
 /* Library options.  "tc_pair": whether tensor-core contractions with

@@ -181,10 +181,10 @@ def test_raster_group_height_does_not_change_results(cuda, engine, rows):
 @pytest.mark.parametrize("engine", ENGINES + ["tc_fp8", "buffer"])
 @pytest.mark.parametrize("ta,tb", [(0, 0), (1, 1), (1, 0)])
 def test_host_buffer_entry_matches_device_path(cuda, engine, ta, tb):
-    # M = 2560: the tensor-core engines pipeline three row blocks (the last ragged);
+    # M = 2300: the tensor-core engines pipeline five row blocks (the last ragged);
     # the SIMT engine takes the plain upload / run / download path
     import torch
-    M, N, K = 2560, 384, 300
+    M, N, K = 2300, 384, 300
     A = oracle.uniform(M * K, seed=5 + ta)
     B = oracle.uniform(K * N, seed=6 + tb)
     C0 = oracle.uniform(M * N, seed=7)
