@@ -197,7 +197,9 @@ int gatlas_matmul_f32_host(const gatlas_matmul_desc *d, const float *A, const fl
  * are bit-identical either way (same pieces, same MMA order, same
  * promotion).  "tc_group_rows": rows of C per raster group of the
  * persistent tensor-core contraction, a multiple of 128 (default 2048): the
- * tiles in flight cover a block of that height, whose operands share L2. */
+ * tiles in flight cover a block of that height, whose operands share L2.
+ * "host_block_rows": rows of A per pipelined block of gatlas_matmul_f32_host,
+ * a multiple of 256 (default 512). */
 int gatlas_set_option(const char *name, int64_t value);
 int gatlas_get_option(const char *name, int64_t *value);
 

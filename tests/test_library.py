@@ -91,3 +91,12 @@ def test_options_round_trip_without_a_device():
     for bad in (0, 100, 129, 65536 + 128):
         with pytest.raises(g.GatlasError, match="multiple of 128"):
             g.set_option("tc_group_rows", bad)
+    assert g.get_option("host_block_rows") == 512
+    g.set_option("host_block_rows", 1024)
+    try:
+        assert g.get_option("host_block_rows") == 1024
+    finally:
+        g.set_option("host_block_rows", 512)
+    for bad in (0, 128, 300):
+        with pytest.raises(g.GatlasError, match="multiple of 256"):
+            g.set_option("host_block_rows", bad)
