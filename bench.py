@@ -767,7 +767,10 @@ def run_tc_sweep(args) -> None:
     """Sustained timing of the tensor-core contraction on prepared operands:
     per size, engine, CTA-pair setting (0 single, 2 pairs) and raster group
     height, about `--sweep-seconds` of back-to-back launches with the SM clock
-    sampled through NVML.  One JSON line per point; cycles = ms x median MHz."""
+    sampled through NVML.  One JSON line per point; cycles = ms x median MHz.
+    Pair settings (gatlas_set_option "tc_pair"): 1 the default choice (CTA
+    pairs for split3/split6, 256 x 256 single-CTA tiles for BF16), 0 single
+    CTAs on 128 x 256 tiles, 2 CTA pairs."""
     import time
 
     import torch
@@ -784,7 +787,7 @@ def run_tc_sweep(args) -> None:
         g.fill(A, "uniform", seed=1)
         g.fill(B, "uniform", seed=2)
         for eng in engines:
-            for pair in (0, 2):
+            for pair in (int(x) for x in args.sweep_pairs.split(",")):
                 g.set_option("tc_pair", pair)
                 ws = torch.empty(g.matmul_workspace_size(M, M, M, eng) + 1024, dtype=torch.uint8, device=dev)
                 ws = ws[(-ws.data_ptr()) % 1024:]
@@ -838,6 +841,7 @@ def main():
     ap.add_argument("--sweep-engines", default="tc_bf16,tc_split3,tc_split6")
     ap.add_argument("--sweep-group-rows", default="2048", help="raster group heights to sweep (multiples of 128)")
     ap.add_argument("--sweep-seconds", type=float, default=1.5)
+    ap.add_argument("--sweep-pairs", default="1,0,2", help="tc_pair settings to sweep")
     args = ap.parse_args()
     if args.tc_sweep:
         run_tc_sweep(args)

@@ -347,8 +347,12 @@ std::ostream &KernelMatmul::print(std::ostream &os) const {
         os << "// tcgen05 kernel tc_gemm_persistent_kernel<" << variant_name(variant_)
            << ">: one CTA per SM over 128x256 output tiles" << (bf16 ? "" : " (CTA pairs over 256x256 tiles when M > 128)")
            << ", TMA " << (split6 ? "64B-swizzled BF16 piece tiles (BK=32)" : "128B-swizzled BF16 piece tiles (BK=64)")
-           << ", tcgen05.mma kind::f16 N=256 K=16, FP32 accumulation in TMEM promoted every "
-           << (extraParam() ? extraParam() : (bf16 ? 8 : 4)) << " K-slices, C stored through TMA\n";
+           << ", tcgen05.mma kind::f16 N=256 K=16, FP32 accumulation in TMEM ";
+        if (bf16 && !extraParam())
+            os << "over all of K (M > 128: tc_gemm_wide_kernel, 256x256 tiles as two M=128 accumulators)";
+        else
+            os << "promoted every " << (extraParam() ? extraParam() : 4) << " K-slices";
+        os << ", C stored through TMA\n";
     } else {
         const size_t bm = groupHeight() * blockHeight(), bn = groupWidth() * blockWidth();
         const bool img = variant_ == Variant::Image;

@@ -779,6 +779,251 @@ __global__ void __launch_bounds__(kThreads2, 1)
 }
 
 // ---------------------------------------------------------------------------
+// Wide contraction (one-product BF16 accumulated over all of K): persistent,
+// one CTA per SM over 256 x 256 tiles, two M = 128 accumulators in all 512
+// TMEM columns.  With no promotion there is nothing to double-buffer: the
+// drain warps stream each tile's accumulators out through the staging tiles
+// and TMA stores, then free TMEM for the next tile (whose K slices the ring
+// has meanwhile prefetched).  The MMA sequence per output element is that of
+// tc_gemm_persistent_kernel<0> with one segment, so the results are
+// bit-identical.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads2, 1)
+    tc_gemm_wide_kernel(const __grid_constant__ CUtensorMap ta0, const __grid_constant__ CUtensorMap tb0,
+                        const __grid_constant__ CUtensorMap tcout, Params p) {
+    using L = WideLayout;
+    constexpr int S = L::STAGES;
+    constexpr int BK = L::BK;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    __shared__ __align__(8) uint64_t full[S], empty[S], tfull, tempty, mma_done;
+    __shared__ uint32_t tmem_base;
+    __shared__ volatile int abort_flag;
+    __shared__ int mma_aborted;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int unit = (int)blockIdx.x, units = (int)gridDim.x;
+    const int64_t per_batch = (int64_t)p.tiles_m * p.tiles_n;
+    const int64_t total = per_batch * p.batch;
+    auto decode = [&](int64_t t, int &tm, int &tn, int &z) {
+        z = (int)(t / per_batch);
+        const int bid = (int)(t - (int64_t)z * per_batch);
+        const int G = p.group_tiles;
+        const int per_group = G * p.tiles_n;
+        const int first_m = (bid / per_group) * G;
+        const int gm = min(p.tiles_m - first_m, G);
+        const int r = bid % per_group;
+        tm = first_m + r % gm;
+        tn = r / gm;
+    };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&tfull, 1);
+        mbar_init(&tempty, kDrainWarps);
+        mbar_init(&mma_done, 1);
+        fence_mbarrier_init();
+        abort_flag = 0;
+        mma_aborted = 0;
+        prefetch_tmap(&ta0);
+        prefetch_tmap(&tb0);
+        if (p.tma_store) prefetch_tmap(&tcout);
+    }
+    if (warp == 0) {
+        tc::tmem_alloc(&tmem_base, kTmemCols2);
+        tc::tmem_relinquish();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_base;
+    auto a_tile = [&](int s) { return smem + s * L::STAGE_BYTES; };
+    auto b_tile = [&](int s) { return smem + s * L::STAGE_BYTES + L::A_TILE; };
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---- TMA producer: one ring position per K slice, across tiles ----
+            int s = 0;
+            uint32_t ph = 0;
+            bool stop = false;
+            for (int64_t t = unit; t < total && !stop; t += units) {
+                int tm, tn, z;
+                decode(t, tm, tn, z);
+                for (int kb = 0; kb < p.kblocks; ++kb) {
+                    if (!tc::wait_timed(&empty[s], ph ^ 1u, kWaitNs, &abort_flag)) {
+                        if (!abort_flag) report_fault(p.fault, kFaultTcProducerWait);
+                        abort_flag = 1;
+                        stop = true;
+                        break;
+                    }
+                    mbar_arrive_expect_tx(&full[s], L::STAGE_BYTES);
+                    tma_load_3d(a_tile(s), &ta0, kb * BK, tm * L::TM, z, &full[s]);
+                    tma_load_3d(b_tile(s), &tb0, kb * BK, tn * BN, z, &full[s]);
+                    if (++s == S) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---- MMA issuer: each tile accumulates over all of K in TMEM ----
+            constexpr uint32_t idesc = L::IDESC;
+            int s = 0;
+            uint32_t ph = 0, tph = 0;
+            bool stop = false;
+            for (int64_t t = unit; t < total && !stop; t += units, tph ^= 1u) {
+                // the drain has read the previous tile's accumulators
+                if (!tc::wait_timed(&tempty, tph ^ 1u, kWaitNs, &abort_flag)) {
+                    if (!abort_flag) report_fault(p.fault, kFaultTcMmaWait);
+                    abort_flag = 1;
+                    stop = true;
+                    break;
+                }
+                tc::fence_after_sync();
+                for (int kb = 0; kb < p.kblocks; ++kb) {
+                    if (!tc::wait_timed(&full[s], ph, kWaitNs, &abort_flag)) {
+                        if (!abort_flag) report_fault(p.fault, kFaultTcMmaWait);
+                        abort_flag = 1;
+                        stop = true;
+                        break;
+                    }
+                    tc::fence_after_sync();
+#pragma unroll
+                    for (int kk = 0; kk < L::KSTEPS; ++kk) {
+                        const uint32_t a_addr = smem_u32(a_tile(s)) + kk * 32;
+                        const uint32_t b_addr = smem_u32(b_tile(s)) + kk * 32;
+                        const uint64_t bd = tc::smem_desc_kmajor(b_addr, L::SBO, L::SWIZZLE);
+                        const uint32_t accum = (kb == 0 && kk == 0) ? 0u : 1u;
+                        tc::mma_bf16(tmem, tc::smem_desc_kmajor(a_addr, L::SBO, L::SWIZZLE), bd, idesc, accum);
+                        tc::mma_bf16(tmem + (uint32_t)BN, tc::smem_desc_kmajor(a_addr + L::A_HALF, L::SBO, L::SWIZZLE),
+                                     bd, idesc, accum);
+                    }
+                    tc::commit_to(&empty[s]);
+                    if (++s == S) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+                if (!stop) tc::commit_to(&tfull);
+            }
+            if (stop) {
+                // every MMA issued before the abort completes before TMEM is freed
+                mma_aborted = 1;
+                tc::commit_to(&mma_done);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---- drain: stream each tile's accumulators out ----
+        // warp (quarter q, half h) reads TMEM lanes 32q..32q+31 of accumulator h:
+        // tile rows 128h + 32q + lane, all 256 columns, in chunks of 32
+        const int quarter = warp & 3, half = (warp - 2) >> 2;
+        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+        uint8_t *stage = smem + L::EPI_OFFSET + (warp - 2) * kEpiTileBytes;
+        const bool vec_ok = (p.ldc % 4 == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0) && (p.stride_c % 4 == 0);
+        uint32_t tph = 0;
+        for (int64_t t = unit; t < total; t += units, tph ^= 1u) {
+            int tm, tn, z;
+            decode(t, tm, tn, z);
+            if (!tc::wait_timed(&tfull, tph, 2 * kWaitNs, &abort_flag)) {
+                if (!abort_flag) report_fault(p.fault, kFaultTcEpilogueWait);
+                abort_flag = 1;
+                break;
+            }
+            tc::fence_after_sync();
+            const int64_t row0 = (int64_t)tm * L::TM + half * 128 + quarter * 32;
+            const int64_t n0 = (int64_t)tn * BN;
+#pragma unroll 1
+            for (int c = 0; c < BN / 32; ++c) {
+                uint32_t r[32];
+                {
+                    uint32_t (&lo)[16] = *reinterpret_cast<uint32_t (*)[16]>(&r[0]);
+                    uint32_t (&hi)[16] = *reinterpret_cast<uint32_t (*)[16]>(&r[16]);
+                    const uint32_t col = tmem + lane_base + (uint32_t)(half * BN + c * 32);
+                    tc::tmem_ld_32x32b_x16(col, lo);
+                    tc::tmem_ld_32x32b_x16(col + 16, hi);
+                    tc::tmem_ld_wait();
+                }
+                if (c == BN / 32 - 1) {
+                    // every accumulator column of this warp is read: TMEM is free
+                    tc::fence_before_sync();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&tempty);
+                }
+                const int64_t col0 = n0 + c * 32;
+                if (p.tma_store) {
+                    if (lane == 0) bulk_wait_read<0>();  // the previous store has read the staging tile
+                    __syncwarp();
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        float v[4];
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) {
+                            const float a = __uint_as_float(r[j * 4 + e]);
+                            v[e] = p.gemm ? __fmaf_rn(p.alpha, a, 0.0f) : a;
+                        }
+                        *reinterpret_cast<float4 *>(stage + lane * 128 + ((j ^ (lane & 7)) << 4)) =
+                            make_float4(v[0], v[1], v[2], v[3]);
+                    }
+                    fence_proxy_async_shared();
+                    __syncwarp();
+                    if (lane == 0 && row0 < p.M && col0 < p.N) {
+                        tma_store_3d(&tcout, stage, (int32_t)col0, (int32_t)row0, z);
+                        bulk_commit();
+                    }
+                } else {
+                    const int64_t row = row0 + lane;
+                    if (row < p.M) {
+                        float *crow = p.C + (int64_t)z * p.stride_c + row * p.ldc;
+#pragma unroll
+                        for (int j = 0; j < 32; j += 4) {
+                            float v[4];
+#pragma unroll
+                            for (int e = 0; e < 4; ++e) {
+                                const int64_t col = col0 + j + e;
+                                const float a = __uint_as_float(r[j + e]);
+                                if (p.gemm) {
+                                    const float bc = (p.beta == 0.0f || col >= p.N) ? 0.0f : p.beta * crow[col];
+                                    v[e] = __fmaf_rn(p.alpha, a, bc);
+                                } else {
+                                    v[e] = a;
+                                }
+                            }
+                            if (vec_ok && col0 + j + 3 < p.N) {
+                                *reinterpret_cast<float4 *>(crow + col0 + j) = make_float4(v[0], v[1], v[2], v[3]);
+                            } else {
+#pragma unroll
+                                for (int e = 0; e < 4; ++e)
+                                    if (col0 + j + e < p.N) crow[col0 + j + e] = v[e];
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        if (lane == 0) bulk_wait<0>();  // this warp's C stores are complete
+        __syncwarp();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (threadIdx.x == 0 && abort_flag) {
+        // copies in flight land (microseconds); the MMAs issued before an abort complete
+        const uint64_t t0 = tc::globaltimer();
+        while (tc::globaltimer() - t0 < 20000000ull) {
+        }
+        if (mma_aborted) tc::wait_timed(&mma_done, 0, kWaitNs, nullptr);
+    }
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, kTmemCols2);
+}
+
+// ---------------------------------------------------------------------------
 // split pass: FP32 -> NP BF16 pieces, K-major [batch][rows][Kp]
 // ---------------------------------------------------------------------------
 struct SplitArgs {
@@ -1190,6 +1435,21 @@ __global__ void __launch_bounds__(128)
     nseg[idx] = s + 1;
 }
 
+// Encodes the tensor map of C for the TMA-store epilogue (32 x 32 boxes,
+// 128-byte swizzle) when C allows it; p.tma_store says whether it did.
+static void c_tensor_map(const Geometry &g, Params &p, CUtensorMap *tcout) {
+    p.tma_store = 0;
+    const bool c_ok = (!p.gemm || p.beta == 0.0f) && aligned_to(p.C, 16) && p.ldc % 4 == 0 &&
+                      (g.batch == 1 || p.stride_c % 4 == 0) && g.N < ((int64_t)1 << 31) && g.M < ((int64_t)1 << 31);
+    if (!c_ok) return;
+    const uint64_t cdims[3] = {(uint64_t)g.N, (uint64_t)g.M, (uint64_t)g.batch};
+    const uint64_t cstr[2] = {(uint64_t)p.ldc * 4, (uint64_t)(g.batch > 1 ? p.stride_c : g.M * p.ldc) * 4};
+    const uint32_t cbox[3] = {32, 32, 1};
+    if (make_tensor_map(tcout, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, p.C, cdims, cstr, cbox,
+                        CU_TENSOR_MAP_SWIZZLE_128B) == GATLAS_OK)
+        p.tma_store = 1;
+}
+
 // Persistent launch: as many CTAs (CTA pairs) as fit on the GPU at once, at
 // most one per tile.  C leaves through a TMA tensor map unless beta is used
 // or C is not 16-byte aligned in rows and instances.
@@ -1210,17 +1470,7 @@ static int launch_persistent(const CUtensorMap *ta, const CUtensorMap *tb, const
     p.batch = (int)g.batch;
     p.group_tiles = std::max(1, g_tc_group_rows / PL::TM);
     CUtensorMap tcout = ta[0];  // unused unless tma_store
-    p.tma_store = 0;
-    const bool c_ok = (!p.gemm || p.beta == 0.0f) && aligned_to(p.C, 16) && p.ldc % 4 == 0 &&
-                      (g.batch == 1 || p.stride_c % 4 == 0) && g.N < ((int64_t)1 << 31) && g.M < ((int64_t)1 << 31);
-    if (c_ok) {
-        const uint64_t cdims[3] = {(uint64_t)g.N, (uint64_t)g.M, (uint64_t)g.batch};
-        const uint64_t cstr[2] = {(uint64_t)p.ldc * 4, (uint64_t)(g.batch > 1 ? p.stride_c : g.M * p.ldc) * 4};
-        const uint32_t cbox[3] = {32, 32, 1};
-        if (make_tensor_map(&tcout, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, p.C, cdims, cstr, cbox,
-                            CU_TENSOR_MAP_SWIZZLE_128B) == GATLAS_OK)
-            p.tma_store = 1;
-    }
+    c_tensor_map(g, p, &tcout);
     cudaLaunchConfig_t cfg = {};
     cfg.blockDim = dim3(kThreads2, 1, 1);
     cfg.dynamicSmemBytes = (size_t)smem;
@@ -1251,6 +1501,38 @@ static int launch_persistent(const CUtensorMap *ta, const CUtensorMap *tb, const
     e = cudaLaunchKernelEx(&cfg, kern, ta[0], ta[1], ta[2], tb[0], tb[1], tb[2], tcout, p);
     if (e != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "tc_gemm_persistent_kernel: %s", cudaGetErrorString(e));
     return check_launch("tc_gemm_persistent_kernel");
+}
+
+// Wide launch (one-product BF16 over all of K): one CTA per SM, at most one
+// per 256 x 256 tile; A and B tensor maps with 256-row boxes.
+static int launch_wide(const Geometry &g, const Plan &pl, const WsPtrs &w, Params p, cudaStream_t stream) {
+    using L = WideLayout;
+    CUtensorMap ta, tb, tcout;
+    const uint64_t row_bytes = (uint64_t)pl.Kp * pl.elem;
+    const uint64_t adims[3] = {(uint64_t)pl.Kp, (uint64_t)g.M, (uint64_t)g.batch};
+    const uint64_t astr[2] = {row_bytes, row_bytes * (uint64_t)g.M};
+    const uint64_t bdims[3] = {(uint64_t)pl.Kp, (uint64_t)g.N, (uint64_t)g.batch};
+    const uint64_t bstr[2] = {row_bytes, row_bytes * (uint64_t)g.N};
+    const uint32_t box[3] = {(uint32_t)L::BK, 256, 1};
+    int rc = make_tensor_map(&ta, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, w.a[0], adims, astr, box, CU_TENSOR_MAP_SWIZZLE_128B);
+    if (!rc) rc = make_tensor_map(&tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, w.b[0], bdims, bstr, box, CU_TENSOR_MAP_SWIZZLE_128B);
+    if (rc) return rc;
+    const int smem = (int)L::SMEM_BYTES;
+    cudaError_t e = cudaFuncSetAttribute(tc_gemm_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "tc wide smem attribute: %s", cudaGetErrorString(e));
+    const int64_t tiles_m = (g.M + L::TM - 1) / L::TM, tiles_n = (g.N + BN - 1) / BN;
+    const int64_t total = tiles_m * tiles_n * g.batch;
+    if (tiles_m * tiles_n > 0x7fffffff || total > ((int64_t)1 << 40))
+        return set_error(GATLAS_ERR_INVALID, "matmul: too many tensor-core tiles");
+    p.tiles_m = (int)tiles_m;
+    p.tiles_n = (int)tiles_n;
+    p.batch = (int)g.batch;
+    p.group_tiles = std::max(1, g_tc_group_rows / L::TM);
+    tcout = ta;  // unused unless tma_store
+    c_tensor_map(g, p, &tcout);
+    const int units = (int)std::min<int64_t>(total, sm_count());
+    tc_gemm_wide_kernel<<<(unsigned)units, kThreads2, smem, stream>>>(ta, tb, tcout, p);
+    return check_launch("tc_gemm_wide_kernel");
 }
 
 template <int MODE>
@@ -1298,6 +1580,9 @@ static int launch_tc(const Geometry &g, const Plan &pl, const WsPtrs &w, float *
     if (MODE == 3 && p.kblocks > kMaxFp8Blocks)
         return set_error(GATLAS_ERR_UNSUPPORTED, "matmul: FP8 engine takes K <= %d", kMaxFp8Blocks * 128);
     if constexpr (MODE != 3) {
+        // one-product BF16 accumulated over all of K: 256 x 256 tiles on single CTAs
+        if (MODE == 0 && g_tc_pair == 1 && g.M > BM && p.seg_kblocks >= p.kblocks)
+            return launch_wide(g, pl, w, p, stream);
         return pair ? launch_persistent<MODE, true>(ta, tb, g, p, stream)
                     : launch_persistent<MODE, false>(ta, tb, g, p, stream);
     } else {

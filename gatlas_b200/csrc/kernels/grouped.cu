@@ -53,11 +53,11 @@ constexpr uint64_t kWaitNs = 2000000000ull;
 constexpr int kPackRows = 128;            // rows per pack item
 // The grouped engine stages 128-byte K slices (its packed tiles carry the
 // 128-byte swizzle) and promotes after the same K as the single-instance
-// engine (512 for one-product BF16, 256 for split3), issuing the same MMA
-// sequence, so that each instance's result is bit-identical to it.
+// engine (all of K for one-product BF16, 256 for split3), issuing the same
+// MMA sequence, so that each instance's result is bit-identical to it.
 template <int MODE>
 using GLayout = tcg::Layout<MODE, kRowBytes>;
-constexpr int grouped_seg_kblocks(int mode) { return (mode == 0 ? 512 : 256) / kBK; }
+constexpr int grouped_seg_kblocks(int mode) { return mode == 0 ? tcg::kSegAll : 256 / kBK; }
 
 // Packed byte offset of 16-byte chunk c of row `row` in K slice kb.
 __device__ __forceinline__ int64_t packed_offset(int64_t row, int kb, int c, int tr, int kt) {

@@ -14,15 +14,17 @@ constexpr int BM = 128, BN = 256;
 
 // Default promotion intervals, in K slices of each mode (selectable per call
 // through the descriptor's extra field): split3 promotes every K = 256
-// (4 slices of 64), split6 every K = 128 (4 slices of 32), one-product BF16
-// every K = 512 (8 slices of 64).  Each promotion is a round trip between
-// the MMA issuer and the drain warps (of both CTAs of a pair); at 8192^3,
-// split3 with K = 256 runs 5 % faster than with K = 128 while its normwise
-// error grows from 3.81e-6 to 3.87e-6.  BF16's longer runs add nothing
-// measurable next to its own input rounding (2^-9).  FP8 accumulates runs of
-// at most 4 equally scaled 128-deep blocks.
+// (4 slices of 64), split6 every K = 128 (4 slices of 32).  Each promotion
+// is a round trip between the MMA issuer and the drain warps (of both CTAs
+// of a pair); at 8192^3, split3 with K = 256 runs 5 % faster than with
+// K = 128 while its normwise error grows from 3.81e-6 to 3.87e-6.
+// One-product BF16 accumulates all of K in TMEM (kSegAll): the tensor core's
+// FP32 accumulation error stays far below BF16's own input rounding (2^-9),
+// and without promotion a 256 x 256 tile fits one CTA.  FP8 accumulates runs
+// of at most 4 equally scaled 128-deep blocks.
+constexpr int kSegAll = 1 << 30;
 __host__ __device__ constexpr int default_seg_kblocks(int mode) {
-    return mode == 0 ? 8 : 4;
+    return mode == 0 ? kSegAll : 4;
 }
 // FP8: most 128-deep blocks per tile (K <= 131072).
 constexpr int kMaxFp8Blocks = 1024;
@@ -147,6 +149,29 @@ struct PersistentLayout {
     static constexpr uint32_t IDESC = MD::SCALED ? tc::idesc_e4m3_f32(TM, 256) : tc::idesc_bf16_f32(TM, 256);
     static_assert(!(MD::SCALED && PAIR), "persistent FP8 runs on single CTAs");
     static_assert(STAGES >= 2, "tensor-core pipeline depth");
+};
+
+// Wide layout (one-product BF16 accumulated over all of K): one CTA computes
+// a 256 x 256 tile as two M = 128 accumulators, all 512 TMEM columns, so a K
+// slice stages 256 rows of A and 256 of B (64 KiB) for 8 MMAs: a third fewer
+// bytes per MMA than a 128 x 256 tile, without a CTA pair's round trips.
+struct WideLayout {
+    static constexpr uint32_t ROW_BYTES = 128;
+    static constexpr int BK = 64;                  // BF16 elements per K slice
+    static constexpr uint32_t SWIZZLE = tc::kSwizzle128B;
+    static constexpr uint32_t SBO = 8 * ROW_BYTES;
+    static constexpr int KSTEPS = (int)(ROW_BYTES / 32);
+    static constexpr int TM = 256;
+    static constexpr uint32_t A_TILE = 256 * ROW_BYTES;  // rows 0..127, then 128..255
+    static constexpr uint32_t A_HALF = 128 * ROW_BYTES;
+    static constexpr uint32_t B_TILE = 256 * ROW_BYTES;
+    static constexpr uint32_t STAGE_BYTES = A_TILE + B_TILE;
+    static constexpr uint32_t BUDGET = 226 * 1024;
+    static constexpr int STAGES = (int)((BUDGET - kEpiBytes - 1024) / STAGE_BYTES);
+    static constexpr uint32_t EPI_OFFSET = STAGES * STAGE_BYTES;
+    static constexpr uint32_t SMEM_BYTES = EPI_OFFSET + kEpiBytes + 1024;  // + alignment slack
+    static constexpr uint32_t IDESC = tc::idesc_bf16_f32(128, 256);
+    static_assert(STAGES >= 3, "wide pipeline depth");
 };
 
 template <int NP>

@@ -135,8 +135,9 @@ int gatlas_matvec_f32_noalloc(const gatlas_matvec_desc *d, const float *A, const
  * the tile fields are ignored and `extra` is the promotion interval: the
  * tensor cores accumulate `extra` K slices in TMEM before the partial sum is
  * added into round-to-nearest FP32 registers.  A slice is K = 64 for TC_BF16
- * and TC_SPLIT3 and K = 32 for TC_SPLIT6; 0 selects K = 512 for TC_BF16,
- * K = 256 for TC_SPLIT3 and K = 128 for TC_SPLIT6.
+ * and TC_SPLIT3 and K = 32 for TC_SPLIT6; 0 selects all of K for TC_BF16
+ * (accumulated in TMEM; with M > 128 on 256 x 256 single-CTA tiles), K = 256
+ * for TC_SPLIT3 and K = 128 for TC_SPLIT6.
  * GATLAS_ENGINE_TC_FP8 quantises each operand to E4M3 with one power-of-two
  * FP32 scale per 128 x 128 block (the smallest power of two s with
  * amax / s <= 448); runs of up to `extra` (0 selects 4) 128-deep blocks
