@@ -157,6 +157,25 @@ def test_cta_pairs_match_single_ctas(cuda, engine, ta, tb, M, N, K, beta):
     assert np.array_equal(single, pair)
 
 
+@pytest.mark.parametrize("ta,tb", [(0, 0), (1, 1)])
+@pytest.mark.parametrize("M,N,K,beta,batch", [(1000, 700, 300, 0.0, 1), (513, 257, 1024, 0.5, 1), (300, 260, 96, 0.0, 3)])
+def test_bf16_wide_tiles_match_single_ctas(cuda, ta, tb, M, N, K, beta, batch):
+    # the default BF16 path for M > 128 (256 x 256 single-CTA tiles, all of K in
+    # TMEM) and 128 x 256 tiles run the same MMA sequence per element
+    A = oracle.uniform(batch * M * K, seed=31 + ta)
+    B = oracle.uniform(batch * K * N, seed=32 + tb)
+    Cin = oracle.uniform(batch * M * N, seed=33)
+    wide = _mm(cuda, A, B, M, N, K, "tc_bf16", ta, tb, gemm=True, Cin=Cin, alpha=1.25, beta=beta, batch=batch)
+    try:
+        g.set_option("tc_pair", 0)
+        single = _mm(cuda, A, B, M, N, K, "tc_bf16", ta, tb, gemm=True, Cin=Cin, alpha=1.25, beta=beta, batch=batch)
+    finally:
+        g.set_option("tc_pair", 1)
+    assert np.array_equal(wide, single)
+    ref = oracle.matmul(A, B, M, N, K, ta, tb, mode=oracle.F64, gemm=1, Cin=Cin, alpha=1.25, beta=beta, packed=batch)
+    assert oracle.normwise_error(wide, ref) <= BUDGET["tc_bf16"]
+
+
 @pytest.mark.parametrize("engine", ENGINES)
 @pytest.mark.parametrize("rows", [128, 384, 65536])
 def test_raster_group_height_does_not_change_results(cuda, engine, rows):
