@@ -1580,8 +1580,11 @@ static int launch_tc(const Geometry &g, const Plan &pl, const WsPtrs &w, float *
     if (MODE == 3 && p.kblocks > kMaxFp8Blocks)
         return set_error(GATLAS_ERR_UNSUPPORTED, "matmul: FP8 engine takes K <= %d", kMaxFp8Blocks * 128);
     if constexpr (MODE != 3) {
-        // one-product BF16 accumulated over all of K: 256 x 256 tiles on single CTAs
-        if (MODE == 0 && g_tc_pair == 1 && g.M > BM && p.seg_kblocks >= p.kblocks)
+        // one-product BF16 accumulated over all of K: 256 x 256 tiles on single
+        // CTAs, once there are at least as many of them as SMs (smaller products
+        // keep the twice as many 128 x 256 tiles; the results are identical)
+        const int64_t wide_tiles = ((g.M + 255) / 256) * ((g.N + BN - 1) / BN) * g.batch;
+        if (MODE == 0 && g_tc_pair == 1 && g.M > BM && p.seg_kblocks >= p.kblocks && wide_tiles >= sm_count())
             return launch_wide(g, pl, w, p, stream);
         return pair ? launch_persistent<MODE, true>(ta, tb, g, p, stream)
                     : launch_persistent<MODE, false>(ta, tb, g, p, stream);

@@ -158,10 +158,12 @@ def test_cta_pairs_match_single_ctas(cuda, engine, ta, tb, M, N, K, beta):
 
 
 @pytest.mark.parametrize("ta,tb", [(0, 0), (1, 1)])
-@pytest.mark.parametrize("M,N,K,beta,batch", [(1000, 700, 300, 0.0, 1), (513, 257, 1024, 0.5, 1), (300, 260, 96, 0.0, 3)])
+@pytest.mark.parametrize("M,N,K,beta,batch", [(4000, 2500, 300, 0.0, 1), (3329, 2817, 520, 0.5, 1),
+                                              (1100, 1000, 96, 0.0, 12)])
 def test_bf16_wide_tiles_match_single_ctas(cuda, ta, tb, M, N, K, beta, batch):
-    # the default BF16 path for M > 128 (256 x 256 single-CTA tiles, all of K in
-    # TMEM) and 128 x 256 tiles run the same MMA sequence per element
+    # the default BF16 path for large products (256 x 256 single-CTA tiles, all
+    # of K in TMEM; at least 148 of them here) and 128 x 256 tiles run the same
+    # MMA sequence per element
     A = oracle.uniform(batch * M * K, seed=31 + ta)
     B = oracle.uniform(batch * K * N, seed=32 + tb)
     Cin = oracle.uniform(batch * M * N, seed=33)
