@@ -1786,7 +1786,7 @@ int host_pipeline(const gatlas_matmul_desc *d, const Geometry &g, const float *h
         if (pitch == width) return cudaMemcpyAsync(dst, src, (size_t)(rows * width) * 4, kind, s);
         return cudaMemcpy2DAsync(dst, pitch * 4, src, pitch * 4, width * 4, rows, kind, s);
     };
-    cudaEvent_t ev_start = event(), ev_b = event(), ev_comp_end = event(), ev_down_end = event();
+    cudaEvent_t ev_start = event(), ev_b = event(), ev_up_end = event(), ev_comp_end = event(), ev_down_end = event();
     std::vector<cudaEvent_t> ev_up(nblk), ev_done(nblk);
     for (int64_t b = 0; b < nblk; ++b) {
         ev_up[b] = event();
@@ -1840,9 +1840,12 @@ int host_pipeline(const gatlas_matmul_desc *d, const Geometry &g, const float *h
                  "download C");
         }
     }
-    // the caller's stream resumes when every role is done (also after an error)
+    // the caller's stream resumes when every role is done (also after an
+    // error, so that no copy into the library's buffers is still in flight)
+    cudaEventRecord(ev_up_end, up);
     cudaEventRecord(ev_comp_end, comp);
     cudaEventRecord(ev_down_end, down);
+    cudaStreamWaitEvent(caller, ev_up_end, 0);
     cudaStreamWaitEvent(caller, ev_comp_end, 0);
     cudaStreamWaitEvent(caller, ev_down_end, 0);
     for (cudaEvent_t e : evs)
