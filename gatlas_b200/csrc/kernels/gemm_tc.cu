@@ -1382,9 +1382,11 @@ static WsPtrs ws_ptrs(const Plan &pl, void *ws) {
     return w;
 }
 
-// CTA pairs (256 x 256 tiles) for M > 128: 1 = where they measure faster on
-// B200 (the split engines: at 8192^3 split3 491 vs 476 and split6 257 vs 242
-// TFLOP/s; BF16 and FP8 run faster as single CTAs), 2 = always, 0 = never.
+// Tiling of C for M > 128 ("tc_pair"): 1 = what measures fastest on B200 --
+// CTA pairs for the split engines (17-19 % fewer cycles per 8192^3 launch
+// than 128 x 256 single CTAs), 256 x 256 single-CTA tiles for one-product
+// BF16 over all of K (35 % fewer), 128 x 256 single CTAs for FP8 (pairs
+// measured 30 % slower); 2 = CTA pairs always; 0 = 128 x 256 always.
 static int g_tc_pair = 1;
 // Rows of C per raster group of the persistent kernels (multiple of 128).
 static int g_tc_group_rows = kGroupM * 128;

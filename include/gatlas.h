@@ -191,12 +191,13 @@ int gatlas_matmul_tc_run(const gatlas_matmul_desc *d, const void *workspace, siz
  * overlap.  Results are bit-identical to gatlas_matmul_f32. */
 int gatlas_matmul_f32_host(const gatlas_matmul_desc *d, const float *A, const float *B, float *C, void *stream);
 
-/* Library options.  "tc_pair": whether tensor-core contractions with
- * M > 128 run as CTA pairs (cta_group::2, a 256 x 256 tile per pair, each
- * CTA staging half of B) or one CTA per 128 x 256 tile: 1 (default) where
- * pairs measure faster (the split3 and split6 engines), 2 always, 0 never.  Results
- * are bit-identical either way (same pieces, same MMA order, same
- * promotion).  "tc_group_rows": rows of C per raster group of the
+/* Library options.  "tc_pair": how tensor-core contractions with M > 128
+ * tile C.  1 (default): CTA pairs (cta_group::2, a 256 x 256 tile per pair,
+ * each CTA staging half of B) for split3 and split6; 256 x 256 tiles on
+ * single CTAs for one-product BF16 over all of K once there are at least as
+ * many such tiles as SMs; one CTA per 128 x 256 tile otherwise.  2: CTA
+ * pairs always.  0: 128 x 256 tiles always.  Results are bit-identical in
+ * every case (same pieces, same MMA order, same promotion).  "tc_group_rows": rows of C per raster group of the
  * persistent tensor-core contraction, a multiple of 128 (default 2048): the
  * tiles in flight cover a block of that height, whose operands share L2.
  * "host_block_rows": rows of A per pipelined block of gatlas_matmul_f32_host,
