@@ -188,3 +188,32 @@ def test_k_limit_of_the_fp8_engine(cuda):
     B = torch.zeros(K * N, device=cuda)
     with pytest.raises(g.GatlasError, match="K <="):
         g.matmul(A, B, M, N, K, engine="tc_fp8")
+
+
+def test_tiles_with_different_segment_plans_in_one_launch(cuda):
+    # every 128-row block of A and every 128-column block of B gets its own
+    # pattern of scales along K, and the instances differ too, so the tiles of
+    # one launch have different numbers of segments; 180 tiles of 128 x 256 put
+    # two tiles on some CTAs of the persistent kernel
+    import torch
+    M, N, K, P = 2304, 1280, 768, 2
+    A, B = _operands(M, N, K, P, seed=41)
+    A2 = A.reshape(P, M, K).copy()
+    B2 = B.reshape(P, K, N).copy()
+    for p in range(P):
+        for rb in range(M // 128):
+            for kb in range(K // 128):
+                A2[p, rb * 128:(rb + 1) * 128, kb * 128:(kb + 1) * 128] *= np.float32(2.0 ** ((kb * (rb + 1) + p) % 4 - 2))
+        for cb in range(N // 128):
+            for kb in range(K // 128):
+                if (kb + cb + p) % 3 == 0:
+                    B2[p, kb * 128:(kb + 1) * 128, cb * 128:(cb + 1) * 128] *= np.float32(0.5)
+    A2, B2 = A2.ravel(), B2.ravel()
+    ws = _prepare(cuda, A2, B2, M, N, K, 0, 0, P)
+    qa, qb, sa, sb = _ws_views(ws, M, N, K, P)
+    C = torch.full((P * M * N,), float("nan"), device=cuda)
+    g.matmul_tc_run(ws, M, N, K, C, engine="tc_fp8", batch=P)
+    torch.cuda.synchronize()
+    assert g.device_faults() == 0
+    ref = oracle.matmul_fp8_dequant(qa, sa, qb, sb, M, N, K, batch=P)
+    assert oracle.normwise_error(C.cpu().numpy(), ref) <= PIPE_TOL
