@@ -246,10 +246,11 @@ extern "C" int gatlas_matmul_f32(const gatlas_matmul_desc *d, const float *A, co
 
 // Host buffers in, host buffer out (the reference's bus-transfer timing
 // modes, GatlasBenchmark.cpp:198-265, as one call).  Tensor-core engines with
-// M >= 2048 and one instance run as a pipeline: B is uploaded and prepared
-// once, then A streams in blocks of 1024 rows whose uploads, preparation,
-// contraction and C downloads overlap on two library streams.  Everything
-// else uploads the operands, runs the engine and downloads C on `stream`.
+// one instance and at least two row blocks (option "host_block_rows", 512 by
+// default) run as a pipeline on three library streams: uploads of B and of
+// the row blocks of A, preparation and contraction of each block as it
+// lands, downloads of each block's rows of C.  Everything else uploads the
+// operands, runs the engine and downloads C on `stream`.
 extern "C" int gatlas_matmul_f32_host(const gatlas_matmul_desc *d, const float *A, const float *B, float *C,
                                       void *stream) {
     using namespace gatlas;
