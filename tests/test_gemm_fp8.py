@@ -217,3 +217,23 @@ def test_tiles_with_different_segment_plans_in_one_launch(cuda):
     assert g.device_faults() == 0
     ref = oracle.matmul_fp8_dequant(qa, sa, qb, sb, M, N, K, batch=P)
     assert oracle.normwise_error(C.cpu().numpy(), ref) <= PIPE_TOL
+
+
+def test_segment_plan_across_bit_words(cuda):
+    # 40 blocks of K: the plan's segment-start bits span two 32-bit words, and
+    # the scales change right at the word boundary and inside both words
+    import torch
+    M, N, K = 256, 512, 40 * 128
+    A, B = _operands(M, N, K, 1, seed=51)
+    A2 = A.reshape(M, K).copy()
+    for kb in (3, 31, 32, 33, 39):
+        A2[:, kb * 128:(kb + 1) * 128] *= np.float32(4.0)
+    A2 = A2.ravel()
+    ws = _prepare(cuda, A2, B, M, N, K, 0, 0, 1)
+    qa, qb, sa, sb = _ws_views(ws, M, N, K, 1)
+    C = torch.full((M * N,), float("nan"), device=cuda)
+    g.matmul_tc_run(ws, M, N, K, C, engine="tc_fp8")
+    torch.cuda.synchronize()
+    assert g.device_faults() == 0
+    ref = oracle.matmul_fp8_dequant(qa, sa, qb, sb, M, N, K)
+    assert oracle.normwise_error(C.cpu().numpy(), ref) <= PIPE_TOL
