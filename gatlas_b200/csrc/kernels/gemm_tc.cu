@@ -1147,12 +1147,17 @@ struct QuantArgs {
 // hit 32 distinct banks.
 __device__ __forceinline__ int qt_index(int r, int w) { return r * 32 + (w ^ ((r >> 2) & 31)); }
 
-__device__ __forceinline__ uint32_t e4m3_pack4(float s, float x0, float x1, float x2, float x3) {
+// x / s for the block scale s, a power of two.  Where 1/s is a normal power
+// of two (r != 0), x * r and x / s are the correctly rounded values of the
+// same real number, hence identical; elsewhere (s subnormal or huge) divide.
+__device__ __forceinline__ float scale_down(float x, float s, float r) { return r != 0.0f ? x * r : __fdiv_rn(x, s); }
+
+__device__ __forceinline__ uint32_t e4m3_pack4(float s, float r, float x0, float x1, float x2, float x3) {
     if (s == 0.0f) return 0u;
-    const uint32_t b0 = __nv_cvt_float_to_fp8(__fdiv_rn(x0, s), __NV_SATFINITE, __NV_E4M3);
-    const uint32_t b1 = __nv_cvt_float_to_fp8(__fdiv_rn(x1, s), __NV_SATFINITE, __NV_E4M3);
-    const uint32_t b2 = __nv_cvt_float_to_fp8(__fdiv_rn(x2, s), __NV_SATFINITE, __NV_E4M3);
-    const uint32_t b3 = __nv_cvt_float_to_fp8(__fdiv_rn(x3, s), __NV_SATFINITE, __NV_E4M3);
+    const uint32_t b0 = __nv_cvt_float_to_fp8(scale_down(x0, s, r), __NV_SATFINITE, __NV_E4M3);
+    const uint32_t b1 = __nv_cvt_float_to_fp8(scale_down(x1, s, r), __NV_SATFINITE, __NV_E4M3);
+    const uint32_t b2 = __nv_cvt_float_to_fp8(scale_down(x2, s, r), __NV_SATFINITE, __NV_E4M3);
+    const uint32_t b3 = __nv_cvt_float_to_fp8(scale_down(x3, s, r), __NV_SATFINITE, __NV_E4M3);
     return b0 | (b1 << 8) | (b2 << 16) | (b3 << 24);
 }
 
@@ -1209,18 +1214,20 @@ __global__ void __launch_bounds__(kQThreads, 2) quant_fp8_kernel(QuantArgs a) {
     for (int w = 1; w < kQThreads / 32; ++w) amax = fmaxf(amax, red[w]);
     // s = 2^ceil(log2(amax / 448)), the smallest power of two with amax / s <= 448:
     // with amax = f * 2^e, f in [0.5, 1), that is 2^(e - 9) for f <= 0.875, else 2^(e - 8)
-    float s = 0.0f;
+    float s = 0.0f, rcp = 0.0f;
     if (amax > 0.0f) {
         int e;
         const float f = frexpf(amax, &e);
-        s = ldexpf(1.0f, e - 9 + (f > 0.875f ? 1 : 0));
+        const int j = e - 9 + (f > 0.875f ? 1 : 0);  // s = 2^j
+        s = ldexpf(1.0f, j);
+        if (isfinite(amax) && j >= -126 && j <= 126) rcp = ldexpf(1.0f, -j);  // 1/s, exact and normal
     }
     if (tid == 0) a.scales[(z * a.rblocks + blockIdx.y) * a.kblocks + blockIdx.x] = s;
     if (!a.transposed) {
 #pragma unroll
         for (int i = 0; i < G; ++i) {
             const int idx = i * kQThreads + tid;
-            qt[qt_index(idx >> 5, idx & 31)] = e4m3_pack4(s, v[i * 4], v[i * 4 + 1], v[i * 4 + 2], v[i * 4 + 3]);
+            qt[qt_index(idx >> 5, idx & 31)] = e4m3_pack4(s, rcp, v[i * 4], v[i * 4 + 1], v[i * 4 + 2], v[i * 4 + 3]);
         }
     } else {
 #pragma unroll
@@ -1230,7 +1237,7 @@ __global__ void __launch_bounds__(kQThreads, 2) quant_fp8_kernel(QuantArgs a) {
             // v[(j*4 + kk)*4 + e] is element (row 4*rq + e, k 4*kq + kk)
 #pragma unroll
             for (int e = 0; e < 4; ++e)
-                qt[qt_index(rq * 4 + e, kq)] = e4m3_pack4(s, v[(j * 4 + 0) * 4 + e], v[(j * 4 + 1) * 4 + e],
+                qt[qt_index(rq * 4 + e, kq)] = e4m3_pack4(s, rcp, v[(j * 4 + 0) * 4 + e], v[(j * 4 + 1) * 4 + e],
                                                           v[(j * 4 + 2) * 4 + e], v[(j * 4 + 3) * 4 + e]);
         }
     }
