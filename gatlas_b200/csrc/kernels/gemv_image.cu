@@ -20,6 +20,8 @@
 // must have 16-byte aligned rows (lda % 4 == 0) and 16-byte aligned bases.
 #include <cuda.h>
 
+#include <algorithm>
+
 #include "../common.cuh"
 #include "../device_state.cuh"
 #include "../tcgen05.cuh"
@@ -367,14 +369,28 @@ int matvec_image_f32(const gatlas_matvec_desc *d, const float *A, const float *x
                              CU_TENSOR_MAP_SWIZZLE_NONE);
     if (rc) return rc;
     const int64_t ncb = (M + CC - 1) / CC;
-    int64_t nseg = ((int64_t)sms * 2 + ncb - 1) / ncb;
-    const int64_t max_seg = (N + CR - 1) / CR;
-    if (nseg > max_seg) nseg = max_seg;
-    if (nseg < 1) nseg = 1;
-    if (nseg > 4096) nseg = 4096;
-    int64_t seg_len = (N + nseg - 1) / nseg;
-    seg_len = (seg_len + CR - 1) / CR * CR;  // whole boxes per segment
-    nseg = (N + seg_len - 1) / seg_len;
+    // Row segments per column block: one CTA per SM at a time runs
+    // ceil(ncb * nseg / sms) rounds of seg_len rows plus a fixed cost per CTA
+    // (ring fill, partial sums; about 128 rows' worth), so pick the segment
+    // count whose rounds waste the least SM time (fewest segments among
+    // equals).  64 column blocks of 16384 rows on 148 SMs: 9 segments in 4
+    // rounds rather than 5 segments in 3 rounds, the last of them one-sixth
+    // full.
+    const int64_t max_seg = std::min<int64_t>((N + CR - 1) / CR, 256);
+    int64_t nseg = 1, seg_len = 0;
+    double best = -1.0;
+    for (int64_t cand = 1; cand <= max_seg; ++cand) {
+        int64_t len = (N + cand - 1) / cand;
+        len = (len + CR - 1) / CR * CR;  // whole boxes per segment
+        const int64_t segs = (N + len - 1) / len;
+        const int64_t rounds = (ncb * segs + sms - 1) / sms;
+        const double eff = (double)(ncb * N) / ((double)sms * (double)rounds * (double)(len + 128));
+        if (eff > best + 1e-3) {
+            best = eff;
+            nseg = segs;
+            seg_len = len;
+        }
+    }
     float *partial = nullptr;
     unsigned *counters = nullptr;
     if (nseg > 1) {
