@@ -290,6 +290,7 @@ static bool gemv_vec_ok(const gatlas_matvec_desc *d, const T *A, const T *x) {
 template <typename T>
 static size_t matvec_ws(const gatlas_matvec_desc *d, const void *A, const void *x) {
     if (!d || !d->trans_a) return 0;
+    if (d->engine == GATLAS_ENGINE_IMAGE) return sizeof(T) == 4 ? matvec_image_ws_bytes(d) : 0;
     const ColsPlan pl = cols_plan<T>(d, gemv_vec_ok<T>(d, (const T *)A, (const T *)x));
     return pl.part_bytes + pl.counter_bytes;
 }

@@ -309,23 +309,49 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
+// Row segments per column block of the column-major kernel.  One CTA per SM
+// at a time runs ceil(ncb * nseg / sms) rounds of seg_len rows plus a fixed
+// cost per CTA (ring fill, partial sums; about 128 rows' worth), so the
+// segment count chosen is the one whose rounds waste the least SM time
+// (fewest segments among equals).  64 column blocks of 16384 rows on 148 SMs:
+// 9 segments in 4 rounds rather than 5 segments in 3 rounds, the last of them
+// one-sixth full.  The workspace query and the launch both call this, so a
+// workspace sized by the query always fits the launch.
+struct ColSegments {
+    int64_t ncb, nseg, seg_len;
+    size_t part_bytes, cnt_bytes;  // both 0 when nseg == 1 (no partial sums)
+};
+
+ColSegments col_segments(int64_t M, int64_t N, int sms) {
+    ColSegments s{(M + CC - 1) / CC, 1, 0, 0, 0};
+    const int64_t max_seg = std::min<int64_t>((N + CR - 1) / CR, 256);
+    double best = -1.0;
+    for (int64_t cand = 1; cand <= max_seg; ++cand) {
+        int64_t len = (N + cand - 1) / cand;
+        len = (len + CR - 1) / CR * CR;  // whole boxes per segment
+        const int64_t segs = (N + len - 1) / len;
+        const int64_t rounds = (s.ncb * segs + sms - 1) / sms;
+        const double eff = (double)(s.ncb * N) / ((double)sms * (double)rounds * (double)(len + 128));
+        if (eff > best + 1e-3) {
+            best = eff;
+            s.nseg = segs;
+            s.seg_len = len;
+        }
+    }
+    if (s.nseg > 1) {
+        s.part_bytes = ((size_t)s.nseg * M * 4 + 255) & ~(size_t)255;
+        s.cnt_bytes = ((size_t)s.ncb * 4 + 255) & ~(size_t)255;
+    }
+    return s;
+}
+
 }  // namespace gvi
 
 size_t matvec_image_ws_bytes(const gatlas_matvec_desc *d) {
     using namespace gvi;
-    if (!d || !d->trans_a || d->n == 0) return 0;
-    const int64_t M = (int64_t)d->m, N = (int64_t)d->n;
-    const int64_t ncb = (M + CC - 1) / CC;
-    int64_t nseg = ((int64_t)sm_count() * 2 + ncb - 1) / ncb;
-    const int64_t max_seg = (N + CR - 1) / CR;
-    if (nseg > max_seg) nseg = max_seg;
-    if (nseg < 1) nseg = 1;
-    if (nseg > 4096) nseg = 4096;
-    int64_t seg_len = (N + nseg - 1) / nseg;
-    seg_len = (seg_len + CR - 1) / CR * CR;
-    nseg = (N + seg_len - 1) / seg_len;
-    if (nseg <= 1) return 0;
-    return (((size_t)nseg * M * 4 + 255) & ~(size_t)255) + (((size_t)ncb * 4 + 255) & ~(size_t)255);
+    if (!d || !d->trans_a || d->n == 0 || d->m == 0) return 0;
+    const ColSegments s = col_segments((int64_t)d->m, (int64_t)d->n, sm_count());
+    return s.part_bytes + s.cnt_bytes;
 }
 
 int matvec_image_f32(const gatlas_matvec_desc *d, const float *A, const float *x, float *y, void *ws,
@@ -368,34 +394,12 @@ int matvec_image_f32(const gatlas_matvec_desc *d, const float *A, const float *x
     int rc = make_tensor_map(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(A), dims, strides, box,
                              CU_TENSOR_MAP_SWIZZLE_NONE);
     if (rc) return rc;
-    const int64_t ncb = (M + CC - 1) / CC;
-    // Row segments per column block: one CTA per SM at a time runs
-    // ceil(ncb * nseg / sms) rounds of seg_len rows plus a fixed cost per CTA
-    // (ring fill, partial sums; about 128 rows' worth), so pick the segment
-    // count whose rounds waste the least SM time (fewest segments among
-    // equals).  64 column blocks of 16384 rows on 148 SMs: 9 segments in 4
-    // rounds rather than 5 segments in 3 rounds, the last of them one-sixth
-    // full.
-    const int64_t max_seg = std::min<int64_t>((N + CR - 1) / CR, 256);
-    int64_t nseg = 1, seg_len = 0;
-    double best = -1.0;
-    for (int64_t cand = 1; cand <= max_seg; ++cand) {
-        int64_t len = (N + cand - 1) / cand;
-        len = (len + CR - 1) / CR * CR;  // whole boxes per segment
-        const int64_t segs = (N + len - 1) / len;
-        const int64_t rounds = (ncb * segs + sms - 1) / sms;
-        const double eff = (double)(ncb * N) / ((double)sms * (double)rounds * (double)(len + 128));
-        if (eff > best + 1e-3) {
-            best = eff;
-            nseg = segs;
-            seg_len = len;
-        }
-    }
+    const ColSegments seg = col_segments(M, N, sms);
+    const int64_t ncb = seg.ncb, nseg = seg.nseg, seg_len = seg.seg_len;
     float *partial = nullptr;
     unsigned *counters = nullptr;
     if (nseg > 1) {
-        const size_t part_bytes = ((size_t)nseg * M * 4 + 255) & ~(size_t)255;
-        const size_t cnt_bytes = ((size_t)ncb * 4 + 255) & ~(size_t)255;
+        const size_t part_bytes = seg.part_bytes, cnt_bytes = seg.cnt_bytes;
         if (!ws) {
             ws = device_scratch(part_bytes + cnt_bytes);
             if (!ws) return set_error(GATLAS_ERR_NOMEM, "matvec: scratch");

@@ -152,3 +152,26 @@ def test_image_engine_full_size_matches_buffer(cuda, ta):
     err = torch.linalg.norm((yi - yb).double()) / torch.linalg.norm(yb.double())
     assert float(err) <= 4 * N * U32
     assert g.device_faults() == 0
+
+
+@pytest.mark.parametrize("engine", ["buffer", "image"])
+@pytest.mark.parametrize("M,N", [(16384, 16384), (4096, 50000), (300, 7000), (1024, 96)])
+def test_workspace_of_the_queried_size_fits(cuda, engine, M, N):
+    """A workspace of exactly gatlas_matvec_workspace_size bytes is accepted by
+    both engines' column-major paths, and gives the same y as library scratch."""
+    import torch
+    A = torch.empty(M * N, dtype=torch.float32, device=cuda)
+    x = torch.empty(N, dtype=torch.float32, device=cuda)
+    g.fill(A, "uniform", seed=M + N)
+    g.fill(x, "uniform", seed=N + 3)
+    need = g.matvec_workspace_size(M, N, trans_a=True)
+    ws = torch.empty(max(need, 1), dtype=torch.uint8, device=cuda)[:need]
+    y_ws = g.matvec(A, x, M, N, trans_a=True, engine=engine, workspace=ws if need else None)
+    y_lib = g.matvec(A, x, M, N, trans_a=True, engine=engine)
+    torch.cuda.synchronize()
+    assert torch.equal(y_ws, y_lib)
+    lo = max(0, M - 48)
+    Aw = A.view(N, M)[:, lo:].contiguous().cpu().numpy().ravel()
+    ref = oracle.matvec(Aw, x.cpu().numpy(), M - lo, N, 1, mode=oracle.F64)
+    assert oracle.normwise_error(y_ws[lo:].cpu().numpy(), ref) <= 4 * N * U32
+    assert g.device_faults() == 0
