@@ -76,7 +76,9 @@ int gatlas_saxpy_f64(int engine, size_t n, double alpha, const double *x, const 
  * KernelMatvecImage.hpp:188-295).  Deterministic: the summation order
  * depends only on (M, N, engine) and the device's SM count.
  * `workspace` may be NULL, in which case the library uses an internal
- * per-device buffer; gatlas_matvec_workspace_size() gives the bytes needed.
+ * per-device buffer; gatlas_matvec_workspace_size() gives the bytes needed
+ * (the most that either engine, float or double, needs for these sizes on
+ * the current device), and a workspace must start on a 256-byte boundary.
  * Calls that use the internal per-device buffers (here, gatlas_matmul_* with
  * no workspace, gatlas_matmul_f32_host) share them: calls on one device that
  * overlap on the GPU (several streams or host threads) race; serialise them or
