@@ -128,7 +128,7 @@ def test_run_time_compiled_points_bit_exact(cuda, ta, tb, tile):
 
 
 def test_full_size_residual_4096(cuda):
-    # FP64 residual on the device against the north-star tolerance 4*K*u
+    # FP64 residual on the device against the normwise tolerance 4*K*u
     import torch
     M = N = K = 4096
     A = torch.empty(M * K, dtype=torch.float32, device=cuda)

@@ -98,7 +98,7 @@ def test_tiled_port_equals_fma_chain():
             assert np.array_equal(ref, til)
 
 
-def test_fma_within_north_star_tolerance_of_f64():
+def test_fma_within_normwise_4ku_of_f64():
     M, N, K = 64, 64, 512
     A = oracle.uniform(M * K, seed=5)
     B = oracle.uniform(K * N, seed=6)
