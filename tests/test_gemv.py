@@ -89,7 +89,7 @@ def test_empty_inner_dimension(cuda):
 
 @pytest.mark.parametrize("ta", [0, 1])
 def test_full_size_16384(cuda, ta):
-    # BASELINE size: A 16384^2 (1 GiB); checked against FP64 on 256 sampled rows
+    # full GEMV workload: A 16384^2 (1 GiB); checked against FP64 on 256 sampled rows
     import torch
     M = N = 16384
     A = torch.empty(M * N, dtype=torch.float32, device=cuda)
