@@ -555,7 +555,7 @@ def run_ours(args, rank, world, local):
         del Ad, Bd, Cd
     del C, ws
 
-    # ---- memory-bound pair: GEMV 16384^2, SAXPY 2^28 -----------------------------------------
+    # ---- memory-bound pair: GEMV 16384^2, SAXPY 2^28
     secondary = {}
     Ag = torch.empty(N_GEMV * N_GEMV, dtype=torch.float32, device=dev)
     xg = torch.empty(N_GEMV, dtype=torch.float32, device=dev)
