@@ -183,11 +183,13 @@ int gatlas_matmul_tc_run(const gatlas_matmul_desc *d, const void *workspace, siz
 
 /* Host buffers in and out: uploads op(A), op(B) (and C when gemm and
  * beta != 0), contracts and downloads C, ordered on `stream` (the call
- * returns before the work completes; synchronise the stream before reading
- * C).  Replaces the reference's bus-transfer timing modes -s/-r
+ * returns before the work completes: keep A, B and C allocated and A and B
+ * unchanged until the stream has completed, and synchronise it before
+ * reading C).  Replaces the reference's bus-transfer timing modes -s/-r
  * (GatlasBenchmark.cpp:198-265).  Tensor-core engines with one instance and
- * M >= 1024 pipeline the transfers on three library streams: uploads (B,
- * then A in blocks of 512 rows, back to back), preparation and contraction
+ * M of at least two blocks (option "host_block_rows", 512 rows by default)
+ * pipeline the transfers on three library streams: uploads (B, then A block
+ * by block, back to back), preparation and contraction
  * of each block as it lands, and the download of each block's C rows as
  * its contraction finishes.  Use pinned host memory for the copies to
  * overlap.  Results are bit-identical to gatlas_matmul_f32. */
@@ -199,8 +201,9 @@ int gatlas_matmul_f32_host(const gatlas_matmul_desc *d, const float *A, const fl
  * single CTAs for one-product BF16 over all of K once there are at least as
  * many such tiles as SMs; one CTA per 128 x 256 tile otherwise.  2: CTA
  * pairs always.  0: 128 x 256 tiles always.  Results are bit-identical in
- * every case (same pieces, same MMA order, same promotion).  "tc_group_rows": rows of C per raster group of the
- * persistent tensor-core contraction, a multiple of 128 (default 2048): the
+ * every case (same pieces, same MMA order, same promotion).
+ * "tc_group_rows": rows of C per raster group of the persistent
+ * tensor-core contraction, a multiple of 128 (default 2048): the
  * tiles in flight cover a block of that height, whose operands share L2.
  * "host_block_rows": rows of A per pipelined block of gatlas_matmul_f32_host,
  * a multiple of 256 (default 512). */
