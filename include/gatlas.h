@@ -164,7 +164,8 @@ typedef struct gatlas_matmul_desc {
 
 /* Bytes of scratch the engine needs (split / quantised operand copies for the
  * TC_* engines, 0 for SIMT).  workspace may be NULL: the library then uses an
- * internal per-device buffer. */
+ * internal per-device buffer; otherwise it is 1024-byte aligned and at least
+ * this size. */
 size_t gatlas_matmul_workspace_size(const gatlas_matmul_desc *d);
 int gatlas_matmul_f32(const gatlas_matmul_desc *d, const float *A, const float *B, float *C,
                       void *workspace, size_t workspace_bytes, void *stream);
