@@ -55,3 +55,27 @@ def test_create_rejects_bad_arguments_before_device_work():
     with pytest.raises(g.GatlasError, match="leading dimension"):
         g.Grouped([dict(m=16, n=16, k=16, lda=8)], engine="tc_split3")
     assert g.grouped_workspace_size([dict(m=-1, n=16, k=16)]) == 0
+
+
+@pytest.mark.parametrize("engine", ["tc_bf16", "tc_split3"])
+def test_create_asks_for_exactly_the_queried_workspace(engine):
+    """A caller's workspace one byte short of the query is rejected with the
+    size create needs, which is the query's; an unaligned one is rejected too
+    (both before any device work)."""
+    import ctypes
+    import re
+    rng = np.random.default_rng(7)
+    inst = [dict(m=int(m), n=int(n), k=int(k)) for m, n, k in rng.integers(1, 900, (25, 3))]
+    need = g.grouped_workspace_size(inst, engine)
+    assert need > 0
+    arr = g._grouped_instances(inst)
+    for i in range(len(inst)):
+        arr[i].a = arr[i].b = arr[i].c = 1 << 20   # never dereferenced: create stops at the size check
+    h = ctypes.c_void_p()
+    L = g.lib()
+    rc = L.gatlas_grouped_create(g._engine(engine), arr, len(inst), ctypes.c_void_p(1 << 20), need - 1, ctypes.byref(h))
+    assert rc == g.ERR_INVALID and not h.value
+    assert int(re.search(r"workspace \d+ < (\d+) bytes", g.last_error()).group(1)) == need
+    rc = L.gatlas_grouped_create(g._engine(engine), arr, len(inst), ctypes.c_void_p((1 << 20) + 256), need,
+                                 ctypes.byref(h))
+    assert rc == g.ERR_INVALID and "1024-byte aligned" in g.last_error()
