@@ -114,3 +114,20 @@ def test_matvec_workspace_query_covers_the_image_engine(M, N):
     need = int(re.search(r"needs (\d+) bytes", g.last_error()).group(1))
     assert need > 1 << 20
     assert g.matvec_workspace_size(M, N, trans_a=True) >= need
+
+
+@pytest.mark.parametrize("engine", ["tc_bf16", "tc_split3", "tc_split6", "tc_fp8"])
+@pytest.mark.parametrize("M,N,K,ta,tb,batch", [(1000, 700, 333, 0, 0, 1), (4096, 4096, 4096, 1, 1, 1),
+                                               (129, 257, 1000, 0, 1, 3), (16, 16, 16, 1, 0, 65535)])
+def test_tc_prepare_asks_for_exactly_the_queried_workspace(engine, M, N, K, ta, tb, batch):
+    """tc_prepare rejects a workspace one byte short of gatlas_matmul_workspace_size
+    with the size it needs, which is the query's (before any device work)."""
+    need = g.matmul_workspace_size(M, N, K, engine, ta, tb, batch)
+    assert need > 0
+    d = g.matmul_desc(M, N, K, ta, tb, engine=engine, batch=batch)
+    p = ctypes.c_void_p(1 << 20)
+    rc = g.lib().gatlas_matmul_tc_prepare(ctypes.byref(d), p, p, p, need - 1, None)
+    assert rc == g.ERR_INVALID
+    assert int(re.search(r"workspace \d+ < (\d+) bytes", g.last_error()).group(1)) == need
+    rc = g.lib().gatlas_matmul_tc_prepare(ctypes.byref(d), p, p, ctypes.c_void_p((1 << 20) + 512), need, None)
+    assert rc == g.ERR_INVALID and "1024-byte aligned" in g.last_error()
