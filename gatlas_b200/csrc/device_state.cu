@@ -9,7 +9,6 @@ namespace gatlas {
 namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-int *g_fault[kMaxDevices] = {nullptr};
 void *g_scratch[kScratchSlots][kMaxDevices] = {{nullptr}};
 size_t g_scratch_bytes[kScratchSlots][kMaxDevices] = {{0}};
 cudaStream_t g_streams[kMaxDevices][kPoolStreams] = {{nullptr}};
@@ -21,18 +20,27 @@ int current_device() {
 }
 }  // namespace
 
+// The fault word lives in this file's device memory, so no call ever
+// allocates it: one int per GPU that loads the library, zero when the module
+// loads.  Host code may not use the name as a device address; the address is
+// looked up once per device with cudaGetSymbolAddress, with that device
+// current.
+namespace {
+__device__ int g_fault_word;
+int *g_fault[kMaxDevices] = {nullptr};
+}  // namespace
+
 int *device_fault_word() {
     const int dev = current_device();
     if (dev < 0) return nullptr;
     std::lock_guard<std::mutex> lk(g_mu);
     if (!g_fault[dev]) {
-        int *p = nullptr;
-        if (cudaMalloc(&p, sizeof(int)) != cudaSuccess) return nullptr;
-        if (cudaMemset(p, 0, sizeof(int)) != cudaSuccess) {
-            cudaFree(p);
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_fault_word) != cudaSuccess || !p) {
+            cudaGetLastError();
             return nullptr;
         }
-        g_fault[dev] = p;
+        g_fault[dev] = static_cast<int *>(p);
     }
     return g_fault[dev];
 }

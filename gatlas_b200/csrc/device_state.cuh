@@ -18,8 +18,9 @@ enum FaultCode : int {
     kFaultSelftestWait = 1 << 6,
 };
 
-// Device pointer to the current device's fault word (allocated and zeroed on
-// first use); nullptr if the allocation failed.
+// Device pointer to the current device's fault word: a file-scope __device__
+// int (zero at module load, never allocated) whose address is looked up on
+// the first use per device; nullptr if that lookup failed.
 int *device_fault_word();
 
 // Current device's cached scratch buffer `slot` of at least `bytes` (grown on

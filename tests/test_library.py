@@ -106,11 +106,12 @@ def test_options_round_trip_without_a_device():
 def test_matvec_workspace_query_covers_the_image_engine(M, N):
     """The allocation-free GEMV states the scratch its column-major TMA path
     needs when that is more than its static array, before any CUDA call; the
-    workspace query must never report less for the same problem."""
+    workspace query must never report less for the same problem.  The operand
+    pointers are NULL: the size check comes first, and any path past it stops
+    at the null-pointer check, so no kernel can launch."""
     lib = g.lib()
     d = g.matvec_desc(M, N, trans_a=True, engine="image")
-    p = ctypes.c_void_p(1 << 20)
-    assert lib.gatlas_matvec_f32_noalloc(ctypes.byref(d), p, p, p, None) == g.ERR_INVALID
+    assert lib.gatlas_matvec_f32_noalloc(ctypes.byref(d), None, None, None, None) == g.ERR_INVALID
     need = int(re.search(r"needs (\d+) bytes", g.last_error()).group(1))
     assert need > 1 << 20
     assert g.matvec_workspace_size(M, N, trans_a=True) >= need

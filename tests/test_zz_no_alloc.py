@@ -7,9 +7,10 @@ and cudaFree imply.  For them the library offers a GEMV that takes its
 scratch (the column-major path's partial sums and arrival counters) from a
 fixed 1 MiB device array inside the library instead of allocating it.
 
-These tests call that entry point through the C ABI and compare it with the
-regular entry point, gatlas_matvec_f32, within the GEMV tolerance used by the
-other tests (normwise 4*N*u), on two calls in a row -- the second call finds
+These tests call that entry point through the C ABI, on both engines (plain
+loads and TMA tiles), and compare it with the regular entry point,
+gatlas_matvec_f32, and with the FP64 oracle, within the GEMV tolerance used by
+the other tests (normwise 4*N*u), on two calls in a row -- the second call finds
 the array holding the first call's partial sums and counters and must clear
 what has to start at zero.  This file is collected last on purpose.
 """
@@ -33,15 +34,18 @@ def _noalloc():
     return fn
 
 
+@pytest.mark.parametrize("engine", ["buffer", "image"])
 @pytest.mark.parametrize("trans_a", [1, 0])
-@pytest.mark.parametrize("M,N", [(4096, 3000), (1024, 16384), (333, 777)])
-def test_noalloc_matches_regular_entry_point(cuda, trans_a, M, N):
+@pytest.mark.parametrize("M,N", [(4096, 3000), (1024, 16384), (332, 776)])
+def test_noalloc_matches_regular_entry_point(cuda, engine, trans_a, M, N):
     import torch
     fn = _noalloc()
-    A = torch.from_numpy(oracle.uniform(M * N, seed=M + N)).to(cuda)
-    x = torch.from_numpy(oracle.uniform(N, seed=N)).to(cuda)
-    y_ref = g.matvec(A, x, M, N, trans_a=trans_a)          # regular entry point
-    d = g.matvec_desc(M, N, trans_a=trans_a)
+    Ah = oracle.uniform(M * N, seed=M + N)
+    xh = oracle.uniform(N, seed=N)
+    A = torch.from_numpy(Ah).to(cuda)
+    x = torch.from_numpy(xh).to(cuda)
+    y_ref = g.matvec(A, x, M, N, trans_a=trans_a, engine=engine)   # regular entry point
+    d = g.matvec_desc(M, N, trans_a=trans_a, engine=engine)
     outs = []
     for _ in range(2):                                      # two calls in a row
         y = torch.full((M,), float("nan"), device=cuda)
@@ -49,26 +53,33 @@ def test_noalloc_matches_regular_entry_point(cuda, trans_a, M, N):
         assert rc == 0, g.last_error()
         torch.cuda.synchronize()
         outs.append(y.cpu().numpy())
+    assert g.device_faults() == 0
     ref = y_ref.cpu().numpy()
+    exact = oracle.matvec(Ah, xh, M, N, trans_a, mode=oracle.F64)
     for y in outs:
         assert np.all(np.isfinite(y))
         assert oracle.normwise_error(y, ref) <= 4 * N * U32
+        assert oracle.normwise_error(y, exact) <= 4 * N * U32
 
 
-def test_noalloc_general_form_two_calls(cuda):
+@pytest.mark.parametrize("engine", ["buffer", "image"])
+def test_noalloc_general_form_two_calls(cuda, engine):
     # y = alpha*A^T x + beta*y, and a different problem on the second call
     import torch
     fn = _noalloc()
     for M, N, seed in ((2048, 5000, 1), (640, 20000, 2)):
-        A = torch.from_numpy(oracle.uniform(M * N, seed=seed)).to(cuda)
-        x = torch.from_numpy(oracle.uniform(N, seed=seed + 10)).to(cuda)
-        y0 = torch.from_numpy(oracle.uniform(M, seed=seed + 20)).to(cuda)
-        y_ref = g.matvec(A, x, M, N, y=y0.clone(), trans_a=True, gemv=True, alpha=0.5, beta=-1.5)
+        Ah, xh, yh = oracle.uniform(M * N, seed=seed), oracle.uniform(N, seed=seed + 10), oracle.uniform(M, seed=seed + 20)
+        A, x, y0 = (torch.from_numpy(t).to(cuda) for t in (Ah, xh, yh))
+        y_ref = g.matvec(A, x, M, N, y=y0.clone(), trans_a=True, gemv=True, alpha=0.5, beta=-1.5, engine=engine)
         y = y0.clone()
-        d = g.matvec_desc(M, N, trans_a=True, gemv=True, alpha=0.5, beta=-1.5)
+        d = g.matvec_desc(M, N, trans_a=True, gemv=True, alpha=0.5, beta=-1.5, engine=engine)
         assert fn(ctypes.byref(d), g._ptr(A), g._ptr(x), g._ptr(y), g._stream()) == 0, g.last_error()
         torch.cuda.synchronize()
-        assert oracle.normwise_error(y.cpu().numpy(), y_ref.cpu().numpy()) <= 4 * N * U32
+        assert g.device_faults() == 0
+        got = y.cpu().numpy()
+        assert oracle.normwise_error(got, y_ref.cpu().numpy()) <= 4 * N * U32
+        exact = oracle.matvec(Ah, xh, M, N, 1, mode=oracle.F64, gemv=1, cin=yh, alpha=0.5, beta=-1.5)
+        assert oracle.normwise_error(got, exact) <= 4 * N * U32
 
 
 def test_noalloc_rejects_null_descriptor():
