@@ -73,7 +73,8 @@ class ServerStats(ctypes.Structure):
     _fields_ = [("budget_bytes", ctypes.c_size_t), ("peak_bytes", ctypes.c_size_t),
                 ("used_bytes", ctypes.c_size_t), ("gemm_batches", ctypes.c_int64),
                 ("batched_gemms", ctypes.c_int64), ("host_busy_ns", ctypes.c_int64),
-                ("iterations", ctypes.c_int64), ("phase_ns", ctypes.c_int64 * 5)]
+                ("iterations", ctypes.c_int64), ("phase_ns", ctypes.c_int64 * 5),
+                ("generate_ns", ctypes.c_int64), ("generate_launches", ctypes.c_int64)]
 
 
 _lib = None
@@ -113,6 +114,9 @@ def lib() -> ctypes.CDLL:
     L.gatlas_matmul_residual_f32.argtypes = [ctypes.POINTER(MatmulDesc), vp, vp, vp,
                                              ctypes.POINTER(ctypes.c_double), vp]
     L.gatlas_device_faults.argtypes = [ctypes.POINTER(ctypes.c_int), i32]
+    L.gatlas_reference_matmul.argtypes = [i32, i32, ctypes.POINTER(MatmulDesc), vp, vp, vp, vp, vp]
+    L.gatlas_reference_matvec.argtypes = [i32, i32, ctypes.POINTER(MatvecDesc), vp, vp, vp, vp, vp]
+    L.gatlas_reference_saxpy.argtypes = [i32, i32, sz, ctypes.c_double, vp, vp, vp, vp]
     L.gatlas_matmul_f32_host.argtypes = [ctypes.POINTER(MatmulDesc), vp, vp, vp, vp]
     L.gatlas_set_option.argtypes = [ctypes.c_char_p, ctypes.c_int64]
     L.gatlas_selftest_bounded_wait.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.POINTER(ctypes.c_int), vp]
@@ -317,6 +321,44 @@ def residual(A, B, C, M, N, K, trans_a=False, trans_b=False, alpha=1.0, stream=N
     return tuple(out)
 
 
+def _scalar(t) -> int:
+    torch = _torch()
+    return 0 if t.dtype == torch.float32 else 1
+
+
+def reference_matmul(A, B, M, N, K, fused=True, Cin=None, trans_a=False, trans_b=False, gemm=False,
+                     alpha=1.0, beta=0.0, batch=1, stream=None):
+    """The paranoid check's device reference product (gatlas_reference_matmul):
+    fused mad chain, or (fused=False) separately rounded products and sums."""
+    torch = _torch()
+    _require_cuda(A, B, Cin)
+    C = torch.empty(batch * M * N, dtype=A.dtype, device=A.device)
+    d = matmul_desc(M, N, K, trans_a, trans_b, gemm, alpha, beta, batch=batch)
+    check(lib().gatlas_reference_matmul(_scalar(A), int(bool(fused)), ctypes.byref(d), _ptr(A), _ptr(B),
+                                        _ptr(Cin), _ptr(C), _stream(stream)))
+    return C
+
+
+def reference_matvec(A, x, M, N, fused=True, yin=None, trans_a=False, gemv=False, alpha=1.0, beta=0.0,
+                     batch=1, stream=None):
+    torch = _torch()
+    _require_cuda(A, x, yin)
+    y = torch.empty(batch * M, dtype=A.dtype, device=A.device)
+    d = matvec_desc(M, N, trans_a, gemv, alpha, beta, batch=batch)
+    check(lib().gatlas_reference_matvec(_scalar(A), int(bool(fused)), ctypes.byref(d), _ptr(A), _ptr(x),
+                                        _ptr(yin), _ptr(y), _stream(stream)))
+    return y
+
+
+def reference_saxpy(alpha, x, y, fused=True, stream=None):
+    torch = _torch()
+    _require_cuda(x, y)
+    z = torch.empty_like(x)
+    check(lib().gatlas_reference_saxpy(_scalar(x), int(bool(fused)), x.numel(), float(alpha), _ptr(x), _ptr(y),
+                                       _ptr(z), _stream(stream)))
+    return z
+
+
 def device_faults(clear=True) -> int:
     v = ctypes.c_int(0)
     check(lib().gatlas_device_faults(ctypes.byref(v), int(clear)))
@@ -510,14 +552,18 @@ def get_option(name: str) -> int:
 
 
 def matmul_host(A, B, M, N, K, C, trans_a=False, trans_b=False, gemm=False, alpha=1.0, beta=0.0,
-                engine="tc_split3", batch=1, extra=0, stream=None):
+                engine="tc_split3", batch=1, extra=0, stream=None, lda=0, ldb=0, ldc=0,
+                stride_a=0, stride_b=0, stride_c=0):
     """C = op(A)op(B) with host (CPU, ideally pinned) float32 tensors: upload,
-    contract and download in one call, ordered on the current CUDA stream."""
+    contract and download in one call, ordered on the current CUDA stream.
+    Leading dimensions and instance strides as in include/gatlas.h (0 = dense);
+    only the M x N elements of each instance of C are written."""
     for t in (A, B, C):
         if t is not None and t.is_cuda:
             raise ValueError("matmul_host takes host tensors")
     d = matmul_desc(M, N, K, trans_a, trans_b, gemm, alpha, beta, engine, batch=batch,
-                    tile=(0, 0, 0, 0, 0, extra))
+                    tile=(0, 0, 0, 0, 0, extra), lda=lda, ldb=ldb, ldc=ldc,
+                    stride_a=stride_a, stride_b=stride_b, stride_c=stride_c)
     check(lib().gatlas_matmul_f32_host(ctypes.byref(d), _ptr(A), _ptr(B), _ptr(C), _stream(stream)))
     return C
 

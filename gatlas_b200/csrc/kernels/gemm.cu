@@ -266,10 +266,19 @@ extern "C" int gatlas_matmul_f32_host(const gatlas_matmul_desc *d, const float *
         if (!dev) return set_error(GATLAS_ERR_NOMEM, "matmul_host: device copies");
         return tcg::host_pipeline(d, g, A, B, C, dev, s);
     }
-    const int64_t a_rows = g.ta ? g.K : g.M, b_rows = g.tb ? g.N : g.K;
-    const size_t a_el = g.K ? (size_t)((g.batch - 1) * g.stride_a + a_rows * g.lda) : 0;
-    const size_t b_el = g.K ? (size_t)((g.batch - 1) * g.stride_b + b_rows * g.ldb) : 0;
-    const size_t c_el = (size_t)((g.batch - 1) * g.stride_c + g.M * g.ldc);
+    // Exact extents: the last stored row of an operand holds only its inner
+    // dimension, so the caller's buffer may end there.  Copies read and write
+    // nothing outside [0, extent) of each host buffer, and C comes back row by
+    // row (ldc may exceed N; padding columns and gaps between instances stay
+    // as the caller left them).
+    const int64_t a_rows = g.ta ? g.K : g.M, a_inner = g.ta ? g.M : g.K;
+    const int64_t b_rows = g.tb ? g.N : g.K, b_inner = g.tb ? g.K : g.N;
+    auto extent = [&](int64_t stride, int64_t rows, int64_t ld, int64_t inner) {
+        return (size_t)((g.batch - 1) * stride + (rows - 1) * ld + inner);
+    };
+    const size_t a_el = g.K ? extent(g.stride_a, a_rows, g.lda, a_inner) : 0;
+    const size_t b_el = g.K ? extent(g.stride_b, b_rows, g.ldb, b_inner) : 0;
+    const size_t c_el = extent(g.stride_c, g.M, g.ldc, g.N);
     auto r1k = [](size_t b) { return (b + 1023) / 1024 * 1024; };
     uint8_t *dev = static_cast<uint8_t *>(device_scratch(r1k(a_el * 4) + r1k(b_el * 4) + r1k(c_el * 4) + 1024, 1));
     if (!dev) return set_error(GATLAS_ERR_NOMEM, "matmul_host: device copies");
@@ -281,8 +290,14 @@ extern "C" int gatlas_matmul_f32_host(const gatlas_matmul_desc *d, const float *
         return check_launch("matmul_host upload");
     const int rc = gatlas_matmul_f32(d, dA, dB, dC, nullptr, 0, stream);
     if (rc) return rc;
-    if (cudaMemcpyAsync(C, dC, c_el * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess)
-        return check_launch("matmul_host download");
+    for (int64_t p = 0; p < g.batch; ++p) {
+        const int64_t off = p * g.stride_c;
+        const cudaError_t e =
+            g.ldc == g.N ? cudaMemcpyAsync(C + off, dC + off, (size_t)(g.M * g.N) * 4, cudaMemcpyDeviceToHost, s)
+                         : cudaMemcpy2DAsync(C + off, g.ldc * 4, dC + off, g.ldc * 4, g.N * 4, g.M,
+                                             cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess) return check_launch("matmul_host download");
+    }
     return GATLAS_OK;
 }
 

@@ -1807,7 +1807,10 @@ int host_pipeline(const gatlas_matmul_desc *d, const Geometry &g, const float *h
         cuda(cudaEventRecord(ev_start, caller), "record");
         for (cudaStream_t s : {up, comp, down}) cuda(cudaStreamWaitEvent(s, ev_start, 0), "wait");
         // uploads: B, then every row block of A (and of C when beta is used), back to back
-        cuda(cudaMemcpyAsync(dB, hB, (size_t)(b_rows * g.ldb) * 4, cudaMemcpyHostToDevice, up), "upload B");
+        // exact extents: the last stored row holds only the inner dimension
+        const int64_t b_inner = g.tb ? g.K : g.N;
+        cuda(cudaMemcpyAsync(dB, hB, (size_t)((b_rows - 1) * g.ldb + b_inner) * 4, cudaMemcpyHostToDevice, up),
+             "upload B");
         cuda(cudaEventRecord(ev_b, up), "record");
         const bool read_c = d->gemm && d->beta != 0.0;
         for (int64_t b = 0; b < nblk; ++b) {
@@ -1817,7 +1820,7 @@ int host_pipeline(const gatlas_matmul_desc *d, const Geometry &g, const float *h
                                        up),
                      "upload A");
             else
-                cuda(cudaMemcpyAsync(dA + r0 * g.lda, hA + r0 * g.lda, (size_t)(rows * g.lda) * 4,
+                cuda(cudaMemcpyAsync(dA + r0 * g.lda, hA + r0 * g.lda, (size_t)((rows - 1) * g.lda + g.K) * 4,
                                      cudaMemcpyHostToDevice, up),
                      "upload A");
             if (read_c)

@@ -3,6 +3,8 @@ into BF16 pieces (3 or 6 products).  Checked against the FP64 oracle: exact on
 the reference's test pattern (C == K), within each engine's error budget on
 uniform[-1,1) inputs, and within 4*K*u when every product is exact (sign*2^e
 inputs, where the BF16 pieces represent the operands exactly)."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -217,6 +219,46 @@ def test_host_buffer_entry_matches_device_path(cuda, engine, ta, tb):
     torch.cuda.synchronize()
     assert g.device_faults() == 0
     assert np.array_equal(hC.numpy(), dev)
+
+
+@pytest.mark.parametrize("engine,M,batch", [("buffer", 300, 2), ("tc_split3", 1100, 1), ("tc_split3", 300, 2),
+                                            ("tc_bf16", 1100, 1)])
+def test_host_buffer_entry_with_padded_strides(cuda, engine, M, batch):
+    """Host buffers sized to their exact extent, lda > K, ldb > N, ldc > N and
+    gaps between instances: the result equals the device entry point on the
+    same layout, and padding columns and gaps of C keep the caller's values."""
+    import torch
+    N, K = 200, 150
+    lda, ldb, ldc = K + 5, N + 3, N + 7
+    sa, sb, sc = lda * M + 11, ldb * K + 13, ldc * M + 17
+    ext = lambda st, rows, ld, inner: (batch - 1) * st + (rows - 1) * ld + inner
+    a_el, b_el, c_el = ext(sa, M, lda, K), ext(sb, K, ldb, N), ext(sc, M, ldc, N)
+    A = oracle.uniform(a_el, seed=31)
+    B = oracle.uniform(b_el, seed=32)
+    C0 = np.full(c_el, 7.25, dtype=np.float32)
+    kw = dict(lda=lda, ldb=ldb, ldc=ldc, stride_a=sa, stride_b=sb, stride_c=sc)
+    d = g.matmul_desc(M, N, K, engine=engine, batch=batch, **kw)
+    dC = torch.from_numpy(C0.copy()).to(cuda)
+    dA, dB = torch.from_numpy(A).to(cuda), torch.from_numpy(B).to(cuda)
+    g.check(g.lib().gatlas_matmul_f32(ctypes.byref(d), g._ptr(dA), g._ptr(dB), g._ptr(dC), None, 0, g._stream()))
+    hC = torch.from_numpy(C0.copy()).pin_memory()
+    g.matmul_host(torch.from_numpy(A).pin_memory(), torch.from_numpy(B).pin_memory(), M, N, K, hC,
+                  engine=engine, batch=batch, **kw)
+    torch.cuda.synchronize()
+    assert g.device_faults() == 0
+    got, want = hC.numpy(), dC.cpu().numpy()
+    assert np.array_equal(got, want)
+    written = np.zeros(c_el, dtype=bool)
+    for p in range(batch):
+        for r in range(M):
+            written[p * sc + r * ldc: p * sc + r * ldc + N] = True
+    assert np.all(got[~written] == 7.25)
+    for p in range(batch):
+        Ap = np.stack([A[p * sa + r * lda: p * sa + r * lda + K] for r in range(M)]).ravel()
+        Bp = np.stack([B[p * sb + r * ldb: p * sb + r * ldb + N] for r in range(K)]).ravel()
+        Cp = np.stack([got[p * sc + r * ldc: p * sc + r * ldc + N] for r in range(M)]).ravel()
+        ref = oracle.matmul(Ap, Bp, M, N, K, mode=oracle.F64)
+        assert oracle.normwise_error(Cp, ref) <= (2.0 ** -7 if engine == "tc_bf16" else 8e-6)
 
 
 def test_host_buffer_entry_small_and_pageable(cuda):
