@@ -91,6 +91,12 @@ void gatlas_kernel_paranoid_check(gatlas_kernel *k) {
     if (k) k->k->paranoidCheck();
 }
 
+void gatlas_kernel_paranoid_fused(gatlas_kernel *k, int fused) {
+    if (k) k->k->paranoidFused(fused != 0);
+}
+
+double gatlas_kernel_last_check(const gatlas_kernel *k) { return k ? k->k->lastCheck() : 0.0; }
+
 int gatlas_bench_run(gatlas_kernel *k, const char *journal, size_t trials, const size_t *params, size_t n,
                      int bus_to_device, int bus_from_device, size_t *usec) {
     if (!k || !params || !usec) return set_error(GATLAS_ERR_INVALID, "bench_run: null argument");

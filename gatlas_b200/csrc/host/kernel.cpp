@@ -264,10 +264,10 @@ bool KernelMatmul::setArgs(bool syncInput) {
         if (cudaMemcpyAsync(Cin_.d, Cin_.h, C_.bytes, cudaMemcpyHostToDevice, s) != cudaSuccess) return false;
         int rc = (e == 4) ? ref_matmul<float>((const float *)A_.d, (const float *)B_.d, (const float *)Cin_.d,
                                               (float *)Cref_.d, P, M, N, K, transposeA(), transposeB(),
-                                              generalizedMatmul(), (float)alpha_, (float)beta_, s)
+                                              generalizedMatmul(), (float)alpha_, (float)beta_, s, paranoid_fused_)
                           : ref_matmul<double>((const double *)A_.d, (const double *)B_.d, (const double *)Cin_.d,
                                                (double *)Cref_.d, P, M, N, K, transposeA(), transposeB(),
-                                               generalizedMatmul(), alpha_, beta_, s);
+                                               generalizedMatmul(), alpha_, beta_, s, paranoid_fused_);
         if (rc || !Cref_.download(s)) return false;
     }
     return sync(s);
@@ -462,10 +462,10 @@ bool KernelMatvec::setArgs(bool syncInput) {
         if (!cin_.upload(0)) return false;
         int rc = (e == 4) ? ref_matvec<float>((const float *)A_.d, (const float *)b_.d, (const float *)cin_.d,
                                               (float *)cref_.d, P, M, N, transposeA(), generalizedMatvec(),
-                                              (float)alpha_, (float)beta_, 0)
+                                              (float)alpha_, (float)beta_, 0, paranoid_fused_)
                           : ref_matvec<double>((const double *)A_.d, (const double *)b_.d, (const double *)cin_.d,
                                                (double *)cref_.d, P, M, N, transposeA(), generalizedMatvec(), alpha_,
-                                               beta_, 0);
+                                               beta_, 0, paranoid_fused_);
         if (rc || !cref_.download(0)) return false;
     }
     return sync(0);
@@ -581,8 +581,9 @@ bool KernelSaxpy::setArgs(bool syncInput) {
     if (paranoid_) {
         if (!zref_.ensure(z_.bytes, true)) return false;
         int rc = (e == 4) ? ref_saxpy<float>((const float *)x_.d, (const float *)y_.d, (float *)zref_.d, n,
-                                             (float)alpha_, 0)
-                          : ref_saxpy<double>((const double *)x_.d, (const double *)y_.d, (double *)zref_.d, n, alpha_, 0);
+                                             (float)alpha_, 0, paranoid_fused_)
+                          : ref_saxpy<double>((const double *)x_.d, (const double *)y_.d, (double *)zref_.d, n, alpha_, 0,
+                                              paranoid_fused_);
         if (rc || !zref_.download(0)) return false;
     }
     return sync(0);

@@ -40,6 +40,13 @@ class KernelInterface {
     virtual bool syncOutput() = 0;
     virtual bool checkOutput(bool printOutput = false) = 0;
     virtual void paranoidCheck() = 0;
+    // arithmetic of the paranoid reference: the generated kernels' fused mad
+    // chain (true, the default) or the reference's separately rounded host
+    // loops (false)
+    virtual void paranoidFused(bool fused) = 0;
+    // absdiff (normwise error for the tensor-core engines and GEMV) of the
+    // last paranoid check
+    virtual double lastCheck() const = 0;
     virtual std::vector<size_t> globalWorkItems() const = 0;
     virtual std::vector<size_t> localWorkItems() const = 0;
     virtual std::ostream &print(std::ostream &os) const = 0;
@@ -79,6 +86,8 @@ class KernelMatmul : public KernelInterface, public MatmulParams {
     bool syncOutput() override;
     bool checkOutput(bool printOutput) override;
     void paranoidCheck() override { paranoid_ = true; }
+    void paranoidFused(bool fused) override { paranoid_fused_ = fused; }
+    double lastCheck() const override { return absdiff_; }
     std::vector<size_t> globalWorkItems() const override { return MatmulParams::globalWorkItems(); }
     std::vector<size_t> localWorkItems() const override { return MatmulParams::localWorkItems(); }
     std::ostream &print(std::ostream &os) const override;
@@ -100,6 +109,7 @@ class KernelMatmul : public KernelInterface, public MatmulParams {
     Variant variant_;
     size_t vl_;
     bool paranoid_ = false;
+    bool paranoid_fused_ = true;
     double alpha_ = 1, beta_ = 1, absdiff_ = 0;
     size_t allocM_ = 0, allocN_ = 0, allocK_ = 0, allocP_ = 0;
     bool allocGemm_ = false;
@@ -120,6 +130,8 @@ class KernelMatvec : public KernelInterface, public MatvecParams {
     bool syncOutput() override;
     bool checkOutput(bool printOutput) override;
     void paranoidCheck() override { paranoid_ = true; }
+    void paranoidFused(bool fused) override { paranoid_fused_ = fused; }
+    double lastCheck() const override { return err_; }
     std::vector<size_t> globalWorkItems() const override { return MatvecParams::globalWorkItems(); }
     std::vector<size_t> localWorkItems() const override { return MatvecParams::localWorkItems(); }
     std::ostream &print(std::ostream &os) const override;
@@ -134,6 +146,7 @@ class KernelMatvec : public KernelInterface, public MatvecParams {
     Variant variant_;
     size_t vl_;
     bool paranoid_ = false;
+    bool paranoid_fused_ = true;
     double alpha_ = 1, beta_ = 1, err_ = 0;
     size_t allocM_ = 0, allocN_ = 0, allocP_ = 0;
     DeviceArray A_, b_, c_, cin_, cref_;
@@ -153,6 +166,8 @@ class KernelSaxpy : public KernelInterface, public SaxpyParams {
     bool syncOutput() override;
     bool checkOutput(bool printOutput) override;
     void paranoidCheck() override { paranoid_ = true; }
+    void paranoidFused(bool fused) override { paranoid_fused_ = fused; }
+    double lastCheck() const override { return absdiff_; }
     std::vector<size_t> globalWorkItems() const override { return SaxpyParams::globalWorkItems(); }
     std::vector<size_t> localWorkItems() const override { return SaxpyParams::localWorkItems(); }
     std::ostream &print(std::ostream &os) const override;
@@ -168,6 +183,7 @@ class KernelSaxpy : public KernelInterface, public SaxpyParams {
     Variant variant_;
     size_t vl_;
     bool paranoid_ = false;
+    bool paranoid_fused_ = true;
     double alpha_ = 1, absdiff_ = 0;
     size_t allocLen_ = 0;
     DeviceArray x_, y_, z_, zref_;

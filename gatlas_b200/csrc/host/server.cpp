@@ -140,6 +140,7 @@ struct Server {
     std::map<float *, std::pair<uint8_t *, size_t>> retained;  // result -> allocation
     int64_t batches = 0, batched_gemms = 0, host_busy_ns = 0, iterations = 0;
     int64_t phase_ns[5] = {0, 0, 0, 0, 0};
+    int64_t generate_ns = 0, generate_launches = 0;
     int device = 0;
 
     cudaEvent_t get_event() {
@@ -240,6 +241,12 @@ int generate(const gatlas_request &r, uint8_t *mem, const Layout &L, cudaStream_
         if (!rc) rc = gatlas_fill_f32(pc, (size_t)r.n, GATLAS_DIST_UNIFORM, sd + 2, 0, 0.0f, s);
     }
     return rc;
+}
+
+// Fill launches generate() makes for a request.
+int generate_launch_count(const gatlas_request &r) {
+    if (r.kind == GATLAS_REQ_SAXPY) return 2;
+    return r.beta != 0.0 ? 3 : 2;
 }
 
 // One request through its single-instance engine call (GEMV, SAXPY, and
@@ -449,7 +456,10 @@ int run_continuous(Server &S, const gatlas_request *rq, int32_t count, gatlas_re
             }
             waiting.pop_front();
             res[r].admit_ns = now;
+            const int64_t g0 = now_ns();
             rc = generate(rq[r], s.mem, s.L, S.prep);
+            S.generate_ns += now_ns() - g0;
+            S.generate_launches += generate_launch_count(rq[r]);
             res[r].status = rc;
             if (rc) {
                 res[r].done_ns = now;
@@ -641,6 +651,8 @@ int gatlas_server_stats(const gatlas_server *srv, gatlas_server_stats_t *out) {
     out->host_busy_ns = S.host_busy_ns;
     out->iterations = S.iterations;
     for (int i = 0; i < 5; ++i) out->phase_ns[i] = S.phase_ns[i];
+    out->generate_ns = S.generate_ns;
+    out->generate_launches = S.generate_launches;
     return GATLAS_OK;
 }
 

@@ -17,6 +17,8 @@
 //    in shared memory, and across the S row segments by the last CTA of each
 //    column block (partials in a workspace, arrival counter per column block).
 // Results are deterministic: the order depends only on (M, N) and the SM count.
+#include <algorithm>
+
 #include "../common.cuh"
 #include "../device_state.cuh"
 
@@ -226,17 +228,15 @@ __global__ void __launch_bounds__(kGemvThreads)
 // ---------------------------------------------------------------------------
 int matvec_image_f32(const gatlas_matvec_desc *d, const float *A, const float *x, float *y, void *ws,
                      size_t ws_bytes, cudaStream_t stream);
-size_t matvec_image_ws_bytes(const gatlas_matvec_desc *d);
+int matvec_image_f64(const gatlas_matvec_desc *d, const double *A, const double *x, double *y, void *ws,
+                     size_t ws_bytes, cudaStream_t stream);
+size_t matvec_image_ws_bytes(const gatlas_matvec_desc *d, size_t elem_bytes);
 
 template <typename T>
 static int matvec_image_dispatch(const gatlas_matvec_desc *d, const T *A, const T *x, T *y, void *ws,
                                  size_t ws_bytes, cudaStream_t stream) {
-    if constexpr (sizeof(T) == 4) {
-        return matvec_image_f32(d, A, x, y, ws, ws_bytes, stream);
-    } else {
-        (void)d, (void)A, (void)x, (void)y, (void)ws, (void)ws_bytes, (void)stream;
-        return set_error(GATLAS_ERR_UNSUPPORTED, "matvec: the image (TMA) engine takes float operands");
-    }
+    if constexpr (sizeof(T) == 4) return matvec_image_f32(d, A, x, y, ws, ws_bytes, stream);
+    else return matvec_image_f64(d, A, x, y, ws, ws_bytes, stream);
 }
 
 struct ColsPlan {
@@ -290,7 +290,7 @@ static bool gemv_vec_ok(const gatlas_matvec_desc *d, const T *A, const T *x) {
 template <typename T>
 static size_t matvec_ws(const gatlas_matvec_desc *d, const void *A, const void *x) {
     if (!d || !d->trans_a) return 0;
-    if (d->engine == GATLAS_ENGINE_IMAGE) return sizeof(T) == 4 ? matvec_image_ws_bytes(d) : 0;
+    if (d->engine == GATLAS_ENGINE_IMAGE) return matvec_image_ws_bytes(d, sizeof(T));
     const ColsPlan pl = cols_plan<T>(d, gemv_vec_ok<T>(d, (const T *)A, (const T *)x));
     return pl.part_bytes + pl.counter_bytes;
 }
@@ -386,7 +386,7 @@ extern "C" size_t gatlas_matvec_workspace_size(const gatlas_matvec_desc *d) {
         if (a > best) best = a;
         if (b > best) best = b;
     }
-    const size_t img = gatlas::matvec_image_ws_bytes(d);
+    const size_t img = std::max(gatlas::matvec_image_ws_bytes(d, 4), gatlas::matvec_image_ws_bytes(d, 8));
     return img > best ? img : best;
 }
 

@@ -38,6 +38,10 @@ def _decl():
     L.gatlas_kernel_print.restype = sz
     L.gatlas_kernel_paranoid_check.argtypes = [vp]
     L.gatlas_kernel_paranoid_check.restype = None
+    L.gatlas_kernel_paranoid_fused.argtypes = [vp, i32]
+    L.gatlas_kernel_paranoid_fused.restype = None
+    L.gatlas_kernel_last_check.argtypes = [vp]
+    L.gatlas_kernel_last_check.restype = ctypes.c_double
     L.gatlas_bench_run.argtypes = [vp, ctypes.c_char_p, sz, psz, sz, i32, i32, psz]
     _declared = True
     return L
@@ -107,8 +111,17 @@ class Kernel:
     def print(self) -> str:
         return self._str(_decl().gatlas_kernel_print)
 
-    def paranoid_check(self) -> None:
+    def paranoid_check(self, fused: bool = True) -> None:
+        """Random inputs and a device reference (paranoidCheck).  fused=False
+        gives the reference the separately rounded arithmetic of the
+        reference's host loops instead of the generated kernels' mad chain."""
         _decl().gatlas_kernel_paranoid_check(self._h)
+        _decl().gatlas_kernel_paranoid_fused(self._h, int(bool(fused)))
+
+    def last_check(self) -> float:
+        """absdiff (normwise error for tensor-core engines and GEMV) of the
+        last paranoid check."""
+        return float(_decl().gatlas_kernel_last_check(self._h))
 
     def bench_run(self, params, trials=1, journal=None, bus_to_device=False,
                   bus_from_device=False) -> int:

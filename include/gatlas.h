@@ -331,6 +331,11 @@ typedef struct gatlas_server_stats_t {
     /* host ns per phase: harvest, admission (incl. operand generation),
      * single launches, GEMM batch tables, GEMM batch launches */
     int64_t phase_ns[5];
+    /* host ns spent inside the operand-generation launches of admission, and
+     * their count: a launch blocks while the device's launch queue is full,
+     * so generation time far above a few microseconds per launch is the
+     * device pushing back, not host work */
+    int64_t generate_ns, generate_launches;
 } gatlas_server_stats_t;
 
 typedef struct gatlas_server gatlas_server;
@@ -361,6 +366,24 @@ int gatlas_fill_f64(double *out, size_t n, int dist, uint64_t seed, uint64_t off
 int gatlas_matmul_residual_f32(const gatlas_matmul_desc *d, const float *A, const float *B,
                                const float *C, double *out_host, void *stream);
 
+/* The paranoid check's device reference (the reference's host check loops,
+ * KernelMatmulBuffer.hpp:108-147, KernelMatvecBuffer.hpp:106-142 and
+ * KernelSaxpyBuffer.hpp:106-121, moved to the GPU, one thread per output
+ * element, accumulating k = 0..K-1 in order).  scalar: 0 float, 1 double.
+ * fused == 0: every product and sum rounded separately, the arithmetic of the
+ * reference's g++ -O2 x86-64 host loops (alpha*acc + beta*c reads c even
+ * when beta == 0); fused != 0: the generated kernels' mad chain
+ * (KernelMatmulBuffer.hpp:302-337, KernelSaxpyBuffer.hpp:186-190), which the
+ * SIMT and image engines reproduce bit for bit.  Dense packed layouts only
+ * (leading dimensions and strides 0 or dense); engine and tiling fields of
+ * the descriptors are ignored. */
+int gatlas_reference_matmul(int scalar, int fused, const gatlas_matmul_desc *d, const void *A, const void *B,
+                            const void *Cin, void *C, void *stream);
+int gatlas_reference_matvec(int scalar, int fused, const gatlas_matvec_desc *d, const void *A, const void *x,
+                            const void *yin, void *y, void *stream);
+int gatlas_reference_saxpy(int scalar, int fused, size_t n, double alpha, const void *x, const void *y, void *z,
+                           void *stream);
+
 /* ---- plugin surface: KernelInterface objects -------------------------------
  * One object per kernel family and -T type, with the reference's parameter
  * vector, validity rules, names, flop counts and work-item shapes
@@ -384,6 +407,14 @@ size_t gatlas_kernel_global_work_items(const gatlas_kernel *k, size_t *out, size
 size_t gatlas_kernel_local_work_items(const gatlas_kernel *k, size_t *out, size_t cap);
 size_t gatlas_kernel_print(const gatlas_kernel *k, char *buf, size_t len);         /* print */
 void gatlas_kernel_paranoid_check(gatlas_kernel *k);                                /* paranoidCheck */
+/* Arithmetic of the paranoid check's reference: fused != 0 (the default) the
+ * generated kernels' mad chain, fused == 0 the reference's separately rounded
+ * host loops (see gatlas_reference_matmul).  The pass rule is the
+ * reference's either way: absdiff < 1/length (OCLAppUtil.hpp:212-264). */
+void gatlas_kernel_paranoid_fused(gatlas_kernel *k, int fused);
+/* absdiff (or, for the tensor-core engines and GEMV, the normwise error) of
+ * the last paranoid check. */
+double gatlas_kernel_last_check(const gatlas_kernel *k);
 /* Bench::run (GatlasBenchmark.cpp:178-289): set params, journal the build and
  * run states when `journal` is a path, set args, time `trials` launches (with
  * the host<->device copies when bus_to_device / bus_from_device), check the

@@ -175,3 +175,90 @@ def test_workspace_of_the_queried_size_fits(cuda, engine, M, N):
     ref = oracle.matvec(Aw, x.cpu().numpy(), M - lo, N, 1, mode=oracle.F64)
     assert oracle.normwise_error(y_ws[lo:].cpu().numpy(), ref) <= 4 * N * U32
     assert g.device_faults() == 0
+
+
+def _exact_matvec(A, x, M, N, ta, gemv=False, yin=None, alpha=1.0, beta=0.0):
+    """y in extended precision (numpy longdouble) from the float64 operands:
+    the reference's host loop (KernelMatvecBuffer.hpp:122-138) evaluated
+    without its own rounding, as the yardstick for both float64 results."""
+    Al = np.asarray(A, dtype=np.longdouble).reshape((N, M) if ta else (M, N))
+    Al = Al.T if ta else Al
+    y = Al @ np.asarray(x, dtype=np.longdouble)
+    if gemv:
+        y = alpha * y + beta * np.asarray(yin, dtype=np.longdouble)
+    return y
+
+
+DGEMV_CASES = [("buffer", 999, 777), ("buffer", 1000, 778), ("image", 1000, 778), ("buffer", 4096, 4096),
+               ("image", 4096, 4096), ("buffer", 334, 20000), ("image", 334, 20000), ("buffer", 20000, 64),
+               ("image", 20000, 64)]
+
+
+@pytest.mark.parametrize("ta", [0, 1])
+@pytest.mark.parametrize("engine,M,N", DGEMV_CASES)
+def test_dgemv_vs_oracle(cuda, ta, engine, M, N):
+    """gatlas_matvec_f64 on both layouts and both engines (the image engine
+    is the reference's doubleimg matvec, KernelMatvecImage.hpp:61-65) against
+    the oracle's float64 host loop (mode FMA, sequential k) and an
+    extended-precision product: both within 4*N*u of the exact value,
+    normwise, with u = 2^-53."""
+    U64 = 2.0 ** -53
+    A = oracle.uniform(M * N, seed=M + 3 * N + ta, dtype=np.float64)
+    x = oracle.uniform(N, seed=N + 5, dtype=np.float64)
+    y = _matvec_f64(cuda, A, x, M, N, ta, engine=engine)
+    exact = _exact_matvec(A, x, M, N, ta)
+    host = oracle.matvec(A, x, M, N, ta, mode=oracle.FMA, dtype=np.float64)
+    assert _normwise(y, exact) <= 4 * N * U64
+    assert _normwise(host, exact) <= 4 * N * U64
+    assert _normwise(y, host) <= 8 * N * U64
+    # the general form with alpha and beta
+    yin = oracle.uniform(M, seed=M + 9, dtype=np.float64)
+    y = _matvec_f64(cuda, A, x, M, N, ta, gemv=True, yin=yin, alpha=0.75, beta=-2.0, engine=engine)
+    assert _normwise(y, _exact_matvec(A, x, M, N, ta, True, yin, 0.75, -2.0)) <= 4 * N * U64
+
+
+@pytest.mark.parametrize("engine", ["buffer", "image"])
+@pytest.mark.parametrize("ta", [0, 1])
+def test_dgemv_known_answer(cuda, ta, engine):
+    M, N = 778, 1032
+    y = _matvec_f64(cuda, np.ones(M * N), np.ones(N), M, N, ta, engine=engine)
+    assert np.all(y == N)
+
+
+@pytest.mark.parametrize("ta", [0, 1])
+def test_double_image_engine_full_size_matches_buffer(cuda, ta):
+    # 16384^2 doubles (2 GiB): the image engine against the buffer engine
+    import torch
+    M = N = 16384
+    A = torch.empty(M * N, dtype=torch.float64, device=cuda)
+    x = torch.empty(N, dtype=torch.float64, device=cuda)
+    g.fill(A, "uniform", seed=33)
+    g.fill(x, "uniform", seed=34)
+    yb = g.matvec(A, x, M, N, trans_a=ta, engine="buffer")
+    yi = g.matvec(A, x, M, N, trans_a=ta, engine="image")
+    torch.cuda.synchronize()
+    err = torch.linalg.norm(yi - yb) / torch.linalg.norm(yb)
+    assert float(err) <= 4 * N * 2.0 ** -53
+    assert g.device_faults() == 0
+
+
+def test_double_image_engine_rejects_odd_rows(cuda):
+    with pytest.raises(g.GatlasError) as e:
+        _matvec_f64(cuda, np.ones(33 * 65), np.ones(65), 33, 65, 0, engine="image")
+    assert e.value.status == g.ERR_UNSUPPORTED
+
+
+def _normwise(y, ref):
+    ref = np.asarray(ref, dtype=np.longdouble)
+    d = np.asarray(y, dtype=np.longdouble) - ref
+    return float(np.sqrt(np.sum(d * d)) / np.sqrt(np.sum(ref * ref)))
+
+
+def _matvec_f64(cuda, A, x, M, N, ta, gemv=False, yin=None, alpha=1.0, beta=0.0, engine="buffer"):
+    import torch
+    y = _gpu(cuda, yin) if yin is not None else torch.zeros(M, dtype=torch.float64, device=cuda)
+    g.matvec(_gpu(cuda, np.asarray(A, np.float64)), _gpu(cuda, np.asarray(x, np.float64)), M, N, y=y,
+             trans_a=ta, gemv=gemv, alpha=alpha, beta=beta, engine=engine)
+    torch.cuda.synchronize()
+    assert g.device_faults() == 0
+    return y.cpu().numpy()

@@ -48,6 +48,8 @@ def test_bench_run_journal_and_checks(cuda, tmp_path, t, p, paranoid):
     ("matvec", "float4", [1, 0, 4096, 4096, 0, 64, 4, 4, 0]),
     ("matvec", "float4", [1, 1, 4096, 2048, 1, 64, 8, 4, 1]),
     ("matvec", "double2", [2, 0, 1024, 512, 1, 64, 2, 2, 0]),
+    ("matvec", "doubleimg", [1, 0, 1024, 512, 1, 64, 2, 2, 0]),
+    ("matvec", "doubleimg", [1, 1, 2048, 1024, 0, 64, 4, 2, 0]),
     ("saxpy", "float4", [1, 1 << 20, 4, 256, 0, 4, 0, 4, 0]),
     ("saxpy", "double2", [1, 1 << 18, 2, 64, 0, 2, 0, 2, 1]),
 ])

@@ -62,9 +62,10 @@ def test_misaligned_and_in_place(cuda, engine, offset):
 
 @pytest.mark.parametrize("engine", ["buffer", "image"])
 def test_full_size_in_place(cuda, engine):
-    # n = 2^26 (256 MiB per operand) checked element by element
+    # the memory-bound workload's full size: n = 2^28 (1 GiB per operand),
+    # in place, checked element by element against fmaf
     import torch
-    n = 1 << 26
+    n = 1 << 28
     x = torch.empty(n, dtype=torch.float32, device=cuda)
     y = torch.empty(n, dtype=torch.float32, device=cuda)
     g.fill(x, "uniform", seed=1)

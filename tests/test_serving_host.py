@@ -10,7 +10,7 @@ import gatlas_b200 as g
 def test_record_layouts_match_the_c_abi():
     assert g.request_dtype().itemsize == 72 and g.request_dtype().fields["arrival_ns"][1] == 64
     assert g.result_dtype().itemsize == 48 and g.result_dtype().fields["result"][1] == 32
-    assert ctypes.sizeof(g.ServerConfig) == 32 and ctypes.sizeof(g.ServerStats) == 96
+    assert ctypes.sizeof(g.ServerConfig) == 32 and ctypes.sizeof(g.ServerStats) == 112
 
 
 def test_create_rejects_bad_configurations():
