@@ -16,10 +16,11 @@ timed iterations.  Timing uses CUDA events on the launching stream, max over
 ranks; N > 1 runs independent replicas (weak scaling, no collective on the
 data path).  Rank 0 prints one JSON line.
 
---impl reference times the reference's own algorithm on the host cores: the
-reference's OpenCL kernels need an OpenCL platform that this machine lacks,
-so its CPU implementation is the oracle port (oracle/), a bounded sample of
-the same workload per step.
+--impl reference times the reference's own kernels on the host cores: its
+generated OpenCL C buffer matmul, emitted by the reference's generators and
+compiled for the host CPU (oracle/_ref), on a bounded sample of the same
+workload per step (bands of work groups of the 8192^3 product).  Where
+oracle/_ref is absent the oracle's port of the same algorithm stands in.
 """
 
 from __future__ import annotations
@@ -439,6 +440,12 @@ def serving_leg(args):
                 row[mode]["host_phase_s"] = dict(zip(("harvest", "admit", "single_launch", "batch_tables",
                                                       "batch_launch"),
                                                      ((a - b) / 1e9 for a, b in zip(st["phase_ns"], st0["phase_ns"]))))
+                # admission's operand-generation launches: time blocked in them
+                # (a full device launch queue) against their count
+                gl = st["generate_launches"] - st0["generate_launches"]
+                gs = (st["generate_ns"] - st0["generate_ns"]) / 1e9
+                row[mode]["admit_generate_s"] = gs
+                row[mode]["admit_generate_us_per_launch"] = gs * 1e6 / gl if gl else None
         row["throughput_ratio"] = row["continuous"]["throughput_rps"] / row["serial"]["throughput_rps"]
         row["p50_ratio"] = row["serial"]["p50_ms"] / row["continuous"]["p50_ms"]
         row["p99_ratio"] = row["serial"]["p99_ms"] / row["continuous"]["p99_ms"]
@@ -598,6 +605,19 @@ def run_ours(args, rank, world, local):
     faults = g.device_faults()
     cpu = cpu_baseline(args.cpu_seconds) if (rank == 0 and world == 1 and not args.no_cpu) else None
 
+    # the memory-bound kernels against measured HBM bandwidth (same roofline
+    # terms as the headline kernel: algorithmic bytes / event time)
+    others = []
+    for key, kern in (("sgemv_Ax_buffer_gbs", "gemv_rows_kernel"), ("sgemv_Atx_buffer_gbs", "gemv_cols_kernel"),
+                      ("sgemv_Ax_image_gbs", "gemv_rows_tma_kernel"), ("sgemv_Atx_image_gbs", "gemv_cols_tma_kernel"),
+                      ("saxpy_buffer_gbs", "saxpy_vec_kernel"), ("saxpy_image_gbs", "saxpy_bulk_kernel")):
+        if key in secondary:
+            others.append({"kernel": kern, "workload": key[:-4], "bound": "hbm", "achieved": round(secondary[key], 1),
+                           "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                           "frac": round(secondary[key] / peaks["hbm_gbs"], 3)})
+    roofline["others"] = others
+    target = _target(sweep, value, fro / refn)
+
     out = {
         "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
@@ -617,16 +637,145 @@ def run_ours(args, rank, world, local):
     }
     if cpu:
         out["cpu_baseline"] = cpu
+    out["target"] = target
+    # last key, so that a reader of only the end of the line sees every leg
+    out["summary"] = _summary(out)
     return out
 
 
+def _target(sweep: dict, headline_tflops: float, headline_err: float) -> dict:
+    """The precision target at 8192^3: the split-BF16 engines against the
+    plain SIMT FP32 kernel, >= 3x its TFLOP/s at equal or better normwise
+    error against the FP64 product (uniform operands)."""
+    simt = sweep.get("buffer_uniform")
+    if not simt:
+        return {}
+    out = {"simt_fp32": {"tflops": round(simt["tflops"], 2), "err": simt["normwise_err"]}}
+    for eng in ("tc_split3", "tc_split6"):
+        row = sweep.get(f"{eng}_uniform")
+        if not row:
+            continue
+        ratio = row["tflops"] / simt["tflops"]
+        out[eng] = {"tflops": round(row["tflops"], 1), "err": row["normwise_err"], "x_simt": round(ratio, 2),
+                    "meets": bool(ratio >= 3.0 and row["normwise_err"] <= simt["normwise_err"])}
+    return out
+
+
+def _summary(o: dict) -> dict:
+    """One compact object with every leg's figures."""
+    r = lambda v, n=1: None if v is None else round(v, n)
+    sec = o.get("secondary") or {}
+    sm = {"headline_tflops": r(o["value"]), "e2e_tflops": r(o["e2e"]["value"]),
+          "tc_frac": r(o["roofline"].get("frac"), 3), "err": o.get("error_vs_fp64", {}).get("normwise")}
+    sm["hbm_frac"] = {k[:-9]: r(v, 3) for k, v in sec.items() if k.endswith("_hbm_frac")}
+    sw = o.get("precision_sweep") or {}
+    sm["sweep_kernel_tflops"] = {k.replace("_uniform", ""): r(v.get("kernel_tflops", v["tflops"]))
+                                 for k, v in sw.items() if not k.endswith("_pow2")}
+    sm["target"] = o.get("target")
+    a = o.get("sgemm_1024_autotune") or {}
+    if a:
+        sm["sgemm_1024"] = {"tflops": r(a["best_tflops"], 2), "tile": list(a["best_tile"].values()),
+                            "err": a["error_vs_fp64"]["normwise"]}
+    gr = o.get("grouped") or {}
+    sm["grouped"] = {e: {"x_per_instance": r(gr[e]["speedup_vs_per_instance"], 2),
+                         "tflops_run": r(gr[e]["tflops_graph_run"])} for e in ("tc_split3", "tc_bf16") if e in gr}
+    sv = o.get("serving") or {}
+    sm["serving"] = {k: {"rps": [r(v["continuous"]["throughput_rps"], 0), r(v["serial"]["throughput_rps"], 0)],
+                         "p99_ms": [r(v["continuous"]["p99_ms"], 2), r(v["serial"]["p99_ms"], 2)]}
+                     for k, v in sv.items() if k.startswith("rate_")}
+    cb = o.get("cpu_baseline") or {}
+    if cb:
+        sm["cpu"] = {"tflops": r(cb["value"], 4), "kind": cb["kind"], "cores": cb["cores"],
+                     "secondary": {k: r(v, 3) for k, v in (cb.get("secondary") or {}).items()}}
+    return sm
+
+
 # ---------------------------------------------------------------------------
-# CPU legs (the oracle port of the reference's algorithm)
+# CPU legs: the reference's own generated kernels on the host cores
 # ---------------------------------------------------------------------------
+#
+# oracle/_ref holds the reference's buffer matmul, matvec and saxpy kernels,
+# emitted by the reference's generators and compiled for the host CPU (mad
+# fused); they run one work group per core at a time (OpenMP over work
+# groups).  Where that library is absent the oracle's port of the buffer
+# kernel's algorithm stands in (kind "port").
+
+REF_SGEMM = "bench_sgemm_8192"    # float4, 16 x 16 work items, 8 x 4 inner blocking, extra 0
+
+
+def _ref_kernels():
+    try:
+        import oracle.ref as R
+        return R if R.available() else None
+    except Exception:
+        return None
+
+
+def _ref_band_rows(R) -> int:
+    k = R.kernel(REF_SGEMM)
+    return k["local"][1] * k["params"][9]   # work-group height x inner blocking height
+
+
+def _ref_sgemm_sample(R, seconds: float, threads: int):
+    """Bands of work groups (128 rows of C each) of the reference's 8192^3
+    buffer kernel that take about `seconds` on the host cores: (A, B, C,
+    bands); A holds only the sampled rows."""
+    import numpy as np
+
+    import oracle
+    K = N = M_GEMM
+    rows = _ref_band_rows(R)
+    B = oracle.uniform(K * N, seed=2)
+    A = oracle.uniform(rows * K, seed=1)
+    Afull = np.zeros(M_GEMM * K, np.float32)   # kernel reads A through its band offset
+    Afull[: rows * K] = A
+    C = np.zeros(M_GEMM * N, np.float32)
+    t0 = time.perf_counter()
+    R.run(REF_SGEMM, Afull, B, C, group_begin=(0, 0), group_end=(0, 1), threads=threads)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    bands = max(1, min(M_GEMM // rows, int(seconds / dt)))
+    Afull[: bands * rows * K] = oracle.uniform(bands * rows * K, seed=1)
+    return Afull, B, C, bands
+
+
+def _ref_secondary(R, threads: int) -> dict:
+    """The reference's memory-bound kernels at the workload sizes (SAXPY
+    n = 2^28 as 2^26 float4; SGEMV 16384^2, both layouts, buffer and image)
+    and its SGEMM 1024^3 point, timed once each after one untimed call."""
+    import numpy as np
+
+    import oracle
+    out = {}
+    n = N_SAXPY
+    X, Y = oracle.uniform(n, seed=5), oracle.uniform(n, seed=6)
+    Z = np.empty_like(X)
+    R.run("bench_saxpy_2p28", X, Y, Z, 0.5, threads=threads)
+    t0 = time.perf_counter()
+    R.run("bench_saxpy_2p28", X, Y, Z, 0.5, threads=threads)
+    out["saxpy_gbs"] = 12.0 * n / (time.perf_counter() - t0) / 1e9
+    del X, Y, Z
+    Ag, xg = oracle.uniform(N_GEMV * N_GEMV, seed=3), oracle.uniform(N_GEMV, seed=4)
+    yg = np.zeros(N_GEMV, np.float32)
+    for kid, key in (("bench_sgemv_n_16384", "sgemv_Ax_buffer_gbs"), ("bench_sgemv_t_16384", "sgemv_Atx_buffer_gbs"),
+                     ("bench_sgemv_img_n_16384", "sgemv_Ax_image_gbs"),
+                     ("bench_sgemv_img_t_16384", "sgemv_Atx_image_gbs")):
+        R.run(kid, Ag, xg, yg, threads=threads)
+        t0 = time.perf_counter()
+        R.run(kid, Ag, xg, yg, threads=threads)
+        out[key] = 4.0 * (N_GEMV * N_GEMV + 2 * N_GEMV) / (time.perf_counter() - t0) / 1e9
+    del Ag, xg, yg
+    m = SGEMM_TUNE_N
+    A1, B1, C1 = oracle.uniform(m * m, seed=1), oracle.uniform(m * m, seed=2), np.zeros(m * m, np.float32)
+    R.run("bench_sgemm_1024", A1, B1, C1, threads=threads)
+    t0 = time.perf_counter()
+    R.run("bench_sgemm_1024", A1, B1, C1, threads=threads)
+    out["sgemm_1024_tflops"] = 2.0 * m ** 3 / (time.perf_counter() - t0) / 1e12
+    return out
+
 
 def _cpu_rows_for(seconds: float, threads: int) -> int:
     """Rows of C whose computation takes about `seconds` on the host cores
-    (from a 16-row pilot), a multiple of 16 in [16, 8192]."""
+    (from a 16-row pilot), a multiple of 16 in [16, 8192] (oracle port)."""
     import oracle
     K = N = M_GEMM
     A = oracle.uniform(16 * K, seed=1)
@@ -639,12 +788,28 @@ def _cpu_rows_for(seconds: float, threads: int) -> int:
 
 
 def cpu_baseline(seconds: float) -> dict:
-    """The reference's buffer-kernel algorithm (one tile per work group, fused
-    mad chain over k) on the host cores, on a bounded sample of the 8192^3
-    workload: the first rows of C, sized to about `seconds` of CPU work."""
+    """The reference's 8192^3 buffer kernel on the host cores, on a bounded
+    sample of the workload: the first bands of work groups, sized to about
+    `seconds` of CPU work; plus the reference's memory-bound kernels and its
+    SGEMM 1024^3 point."""
     import oracle
     threads = oracle.max_threads()
     K = N = M_GEMM
+    R = _ref_kernels()
+    if R is not None:
+        A, B, C, bands = _ref_sgemm_sample(R, seconds, threads)
+        rows = bands * _ref_band_rows(R)
+        t0 = time.perf_counter()
+        R.run(REF_SGEMM, A, B, C, group_begin=(0, 0), group_end=(0, bands), threads=threads)
+        dt = time.perf_counter() - t0
+        del A, B, C
+        flops = 2.0 * rows * N * K
+        return {"value": flops / dt / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": "reference",
+                "sample": f"{rows} of 8192 rows of C ({bands} bands of work groups) of the reference's "
+                          f"matmulbufferfloat4 (16x16 work items, 8x4 blocking) at 8192^3: "
+                          f"{flops / 1e9:.0f} GFLOP in {dt:.1f} s",
+                "kernels": "oracle/_ref: the reference's emitted OpenCL C compiled for the host, mad fused",
+                "secondary": _ref_secondary(R, threads)}
     rows = _cpu_rows_for(seconds, threads)
     A = oracle.uniform(rows * K, seed=1)
     B = oracle.uniform(K * N, seed=2)
@@ -665,15 +830,29 @@ def run_reference(args, rank, world):
     K = N = M_GEMM
     # each step a bounded sample sized so the whole run takes a few minutes
     per_step_s = max(1.0, min(8.0, 150.0 / max(1, args.steps + args.warmup)))
-    rows = _cpu_rows_for(per_step_s, threads)
-    A = oracle.uniform(rows * K, seed=1)
-    B = oracle.uniform(K * N, seed=2)
+    R = _ref_kernels()
+    if R is not None:
+        A, B, C, bands = _ref_sgemm_sample(R, per_step_s, threads)
+        rows = bands * _ref_band_rows(R)
+        step = lambda: R.run(REF_SGEMM, A, B, C, group_begin=(0, 0), group_end=(0, bands), threads=threads)
+        kind = "reference"
+        engine = ("the reference's matmulbufferfloat4 kernel (emitted by its generator, 16x16 work items, "
+                  "8x4 blocking) compiled for the host cores, mad fused (oracle/_ref)")
+        sample = f"{rows} of 8192 rows of C ({bands} bands of work groups) of the 8192^3 SGEMM per step"
+    else:
+        rows = _cpu_rows_for(per_step_s, threads)
+        A = oracle.uniform(rows * K, seed=1)
+        B = oracle.uniform(K * N, seed=2)
+        step = lambda: oracle.matmul_tiled(A, B, rows, N, K, tile_m=128, tile_n=64, threads=threads)
+        kind = "port"
+        engine = "the reference's buffer-kernel algorithm on the host cores (oracle port)"
+        sample = f"{rows} of 8192 rows of C of the 8192^3 SGEMM per step"
     for _ in range(min(args.warmup, 1)):
-        oracle.matmul_tiled(A, B, min(rows, 16), N, K, tile_m=16, tile_n=64, threads=threads)
+        step()
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        oracle.matmul_tiled(A, B, rows, N, K, tile_m=128, tile_n=64, threads=threads)
+        step()
         times.append(time.perf_counter() - t0)
     dt = sum(times) / len(times)
     flops = 2.0 * rows * N * K
@@ -684,10 +863,8 @@ def run_reference(args, rank, world):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "impl": "reference",
         "data": "synthetic (seeded uniform[-1,1) FP32 operands)",
         "config": {"workload": "sgemm_fp32_accurate_8192", "m": M_GEMM, "n": M_GEMM, "k": M_GEMM,
-                   "engine": "the reference's buffer-kernel algorithm on the host cores "
-                             "(oracle port; the reference needs an OpenCL platform)"},
-        "cpu_baseline": {"value": v, "unit": "TFLOP/s", "cores": threads, "kind": "port",
-                         "sample": f"{rows} of 8192 rows of C of the 8192^3 SGEMM per step"},
+                   "engine": engine},
+        "cpu_baseline": {"value": v, "unit": "TFLOP/s", "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 

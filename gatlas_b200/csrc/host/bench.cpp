@@ -1,4 +1,12 @@
 // Journal, Bench::run and AppUtil; see bench.hpp for the reference citations.
+//
+// The journal's file format and key format, the run states, the printed
+// status lines and the statistics (Welford mean and variance, top-N pruning,
+// ranking) restate GATLAS's GatlasBenchmark.cpp and GatlasAppUtil.cpp
+// (Copyright 2010 Chris Jang), which are free software under the GNU Lesser
+// General Public License, version 3 or later (the reference's
+// COPYING.LESSER); the formats are kept byte for byte so that journals and
+// tool output interoperate with the reference's.
 #include "bench.hpp"
 
 #include <cmath>
@@ -201,64 +209,72 @@ static void print_point(const std::vector<size_t> &args, const std::vector<size_
     std::cout << ")" << std::endl;
 }
 
+namespace {
+
+// One candidate's time for this trial: a new point is run on the device; a
+// point the journal recorded as good replays its recorded time for this
+// trial (run only if the journal has no time for it); a point the journal
+// recorded mid-build or mid-run (a crash or hang) scores 0 without running.
+size_t trial_time(size_t trial, KernelInterface &kernel, Bench &bench, const Journal *journal, int memoState,
+                  const std::vector<size_t> &args, bool toDevice, bool fromDevice, bool printDebug) {
+    if (memoState == Journal::MISSING) return bench.run(1, args, toDevice, fromDevice, printDebug);
+    kernel.setParams(args);
+    if (memoState != Journal::RUN_OK) {
+        if (bench.printStatus()) std::cout << "bad";
+        return 0;
+    }
+    const int memo = journal->memoTime(kernel, args, trial);
+    return memo == -1 ? bench.run(1, args, toDevice, fromDevice, printDebug) : (size_t)memo;
+}
+
+// Running GFLOPS mean and variance over the trials (Welford's update).
+void accumulate(size_t trial, double rate, double &mean, double &var) {
+    if (trial == 0) {
+        mean = rate;
+        return;
+    }
+    const double delta = rate - mean;
+    mean += delta / (double)(trial + 1);
+    var += (double)trial / (double)(trial + 1) * delta * delta;
+}
+
+}  // namespace
+
 size_t benchLoop(size_t trialNumber, KernelInterface &kernel, Bench &bench, Journal *journal,
                  const std::vector<std::vector<size_t>> &pargs, std::vector<bool> &pargsOk,
                  std::vector<size_t> &pargsTime, std::vector<size_t> &pargsFlops, std::vector<double> &pargsAverage,
                  std::vector<double> &pargsVariance, std::vector<std::vector<size_t>> &pargsExtraDetail,
                  bool busToDevice, bool busFromDevice, bool dummyRun, bool printDebug) {
-    const bool printStatus = bench.printStatus();
+    const bool status = bench.printStatus();
+    bool warmed = !dummyRun;  // one untimed launch before the first point that really runs
     size_t good = 0;
-    bool needDummy = dummyRun;
     for (size_t j = 0; j < pargs.size(); ++j) {
-        const std::vector<size_t> &args = pargs[j];
         if (!pargsOk[j]) continue;
+        const std::vector<size_t> &args = pargs[j];
         const int memoState = journal ? journal->memoRunState(kernel, args) : (int)Journal::MISSING;
-        if (needDummy && memoState == Journal::MISSING) {
+        if (!warmed && memoState == Journal::MISSING) {
             std::cout << "[dummy run] ";
             bench.run(1, args, busToDevice, busFromDevice, printDebug);
             std::cout << std::endl;
-            needDummy = false;
+            warmed = true;
         }
-        if (printStatus) std::cout << "[trial " << trialNumber << "] ";
-        size_t usec;
-        if (memoState == Journal::MISSING) {
-            usec = bench.run(1, args, busToDevice, busFromDevice, printDebug);
-        } else if (memoState == Journal::RUN_OK) {
-            // replay the recorded time for this trial without touching the device
-            const int memo = journal->memoTime(kernel, args, trialNumber);
-            usec = (memo == -1) ? bench.run(1, args, busToDevice, busFromDevice, printDebug) : (size_t)memo;
-            kernel.setParams(args);
+        if (status) std::cout << "[trial " << trialNumber << "] ";
+        const size_t usec =
+            trial_time(trialNumber, kernel, bench, journal, memoState, args, busToDevice, busFromDevice, printDebug);
+        pargsExtraDetail[j] = kernel.extraParamDetail();
+        if (usec > 0) {
+            const size_t nflops = kernel.numberFlops();
+            pargsTime[j] += usec;
+            pargsFlops[j] += nflops;
+            accumulate(trialNumber, (double)nflops / (double)usec / 1000.0, pargsAverage[j], pargsVariance[j]);
+            ++good;
         } else {
-            // crashed while building or hung while running earlier
-            if (printStatus) std::cout << "bad";
-            usec = 0;
-            kernel.setParams(args);
+            pargsOk[j] = false;  // pruned from every later trial
         }
-        const std::vector<size_t> &extra = pargsExtraDetail[j] = kernel.extraParamDetail();
-        if (usec == 0) {
-            if (printStatus) {
-                std::cout << "\t";
-                print_point(args, extra);
-            }
-            pargsOk[j] = false;
-            continue;
-        }
-        ++good;
-        const size_t nflops = kernel.numberFlops();
-        pargsTime[j] += usec;
-        pargsFlops[j] += nflops;
-        // single-pass (Welford) mean and variance of the per-trial GFLOPS
-        const double rate = (double)nflops / usec / 1000;
-        if (trialNumber == 0) {
-            pargsAverage[j] = rate;
-        } else {
-            const double delta = rate - pargsAverage[j];
-            pargsAverage[j] += (1.0 / (trialNumber + 1)) * delta;
-            pargsVariance[j] += ((double)trialNumber / (trialNumber + 1)) * delta * delta;
-        }
-        if (printStatus) {
-            std::cout << usec << "\t";
-            print_point(args, extra);
+        if (status) {
+            if (usec > 0) std::cout << usec;
+            std::cout << "\t";
+            print_point(args, pargsExtraDetail[j]);
         }
     }
     return good;
