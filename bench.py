@@ -872,9 +872,10 @@ def run_reference(args, rank, world):
 def run_case(spec: str) -> None:
     """Small single-kernel cases for ncu captures: NAME:SIZE, three calls each.
     tc_bf16|tc_split3|tc_split6|tc_fp8[_pair]:M (M^3 GEMM, prepare once, run x3; _pair forces CTA pairs),
-    sgemm_simt:M, sgemm_image:M,
-    quant_fp8:M (the FP8 operand pass, x3),
-    gemv_A:N / gemv_At:N (N^2 GEMV), saxpy_buffer:n / saxpy_image:n,
+    sgemm_simt:M, sgemm_image:M, dgemm_simt:M (M^3 float64 on the SIMT engine),
+    quant_fp8:M (the FP8 operand pass, x3), split3_prepare:M (the split-BF16 operand pass, x3),
+    gemv_A:N / gemv_At:N (N^2 GEMV, buffer engine), gemv_img_A:N / gemv_img_At:N (TMA engine),
+    dgemv_A:N / dgemv_At:N / dgemv_img_A:N / dgemv_img_At:N (float64), saxpy_buffer:n / saxpy_image:n,
     grouped_tc_split3|grouped_tc_bf16:count (the batched workload)."""
     import torch
 
@@ -887,7 +888,26 @@ def run_case(spec: str) -> None:
         gb.set_option("tc_pair", 2)
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    if name.startswith("tc_") or name in ("sgemm_simt", "sgemm_image", "quant_fp8"):
+    if name == "dgemm_simt":
+        M = size
+        A = torch.empty(M * M, dtype=torch.float64, device=dev)
+        B = torch.empty(M * M, dtype=torch.float64, device=dev)
+        C = torch.empty(M * M, dtype=torch.float64, device=dev)
+        g.fill(A, "uniform", seed=1)
+        g.fill(B, "uniform", seed=2)
+        for _ in range(3):
+            g.matmul(A, B, M, M, M, C=C)
+    elif name == "split3_prepare":
+        M = size
+        A = torch.empty(M * M, device=dev)
+        B = torch.empty(M * M, device=dev)
+        g.fill(A, "uniform", seed=1)
+        g.fill(B, "uniform", seed=2)
+        ws = torch.empty(g.matmul_workspace_size(M, M, M, "tc_split3") + 1024, dtype=torch.uint8, device=dev)
+        ws = ws[(-ws.data_ptr()) % 1024:]
+        for _ in range(3):
+            g.matmul_tc_prepare(A, B, M, M, M, ws, engine="tc_split3")
+    elif name.startswith("tc_") or name in ("sgemm_simt", "sgemm_image", "quant_fp8"):
         M = size
         A = torch.empty(M * M, device=dev)
         B = torch.empty(M * M, device=dev)
@@ -911,15 +931,17 @@ def run_case(spec: str) -> None:
             g.matmul_tc_prepare(A, B, M, M, M, ws, engine=name)
             for _ in range(3):
                 g.matmul_tc_run(ws, M, M, M, C, engine=name)
-    elif name.startswith("gemv_"):
+    elif name.startswith("gemv_") or name.startswith("dgemv_"):
         N = size
-        A = torch.empty(N * N, device=dev)
-        x = torch.empty(N, device=dev)
-        y = torch.empty(N, device=dev)
+        dt = torch.float64 if name.startswith("d") else torch.float32
+        A = torch.empty(N * N, dtype=dt, device=dev)
+        x = torch.empty(N, dtype=dt, device=dev)
+        y = torch.empty(N, dtype=dt, device=dev)
         g.fill(A, "uniform", seed=1)
         g.fill(x, "uniform", seed=2)
+        eng = "image" if "_img_" in name else "buffer"
         for _ in range(3):
-            g.matvec(A, x, N, N, y=y, trans_a=(name == "gemv_At"))
+            g.matvec(A, x, N, N, y=y, trans_a=name.endswith("_At"), engine=eng)
     elif name.startswith("saxpy_"):
         x = torch.empty(size, device=dev)
         y = torch.empty(size, device=dev)
