@@ -7,10 +7,13 @@
 // row-major A.
 //
 // B200 design (both layouts read every byte of A exactly once, 16-byte loads):
-//  * trans_a == 0 (row-major): a warp owns ROWS rows at a time; lanes stride
-//    across the row in 16-byte vectors with UNROLL loads per row in flight,
-//    fused multiply-add chains per lane, then a fixed butterfly shuffle
-//    reduction.  x is read through the L1-cached read-only path.
+//  * trans_a == 0 (row-major): for long rows (at least 4 x 256 vectors) a CTA
+//    owns two rows at a time and its 256 threads stride across them in
+//    16-byte vectors, reduced in a fixed order (warp butterfly, then the 8
+//    warps in shared memory); otherwise a warp owns ROWS rows at a time, its
+//    lanes striding across the row with UNROLL loads per row in flight and a
+//    fixed butterfly shuffle reduction.  x is read through the L1-cached
+//    read-only path.
 //  * trans_a == 1 (column-major): a CTA owns 32*VW adjacent columns (one
 //    16-byte vector per lane) and one segment of the rows; its 8 warps take
 //    interleaved rows, partial sums are combined across warps in a fixed order
@@ -127,6 +130,75 @@ __global__ void __launch_bounds__(kGemvThreads)
             const size_t row = row0 + lane;
             if (row < a.M) y[row] = epilogue<T>(a.gemv, alpha, beta, v, y + row);
         }
+    }
+}
+
+// Long rows: a CTA owns RB rows at a time and all 256 threads stride across
+// each of them in 16-byte vectors (UNROLL per row in flight, x reused from
+// registers across the RB rows); the per-thread chains are combined by a
+// fixed butterfly per warp and a fixed-order sum over the 8 warps in shared
+// memory.  The units are 8 times smaller than a warp's rows, so a 16384^2
+// product is thousands of CTAs and the last partial wave costs little.
+template <typename T, int VW, int RB, int UNROLL>
+__global__ void __launch_bounds__(kGemvThreads)
+    gemv_rowblock_kernel(GemvArgs a) {
+    using V = typename VecT<T, VW>::type;
+    __shared__ T red[RB][kGemvWarps];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const size_t p = blockIdx.y;
+    const T *A = static_cast<const T *>(a.A) + p * a.stride_a;
+    const V *x = reinterpret_cast<const V *>(static_cast<const T *>(a.x) + p * a.stride_x);
+    T *y = static_cast<T *>(a.y) + p * a.stride_y;
+    const size_t nvec = a.N / VW;
+    const T alpha = (T)a.alpha, beta = (T)a.beta;
+    const size_t nblocks = (a.M + RB - 1) / RB;
+    for (size_t rb = blockIdx.x; rb < nblocks; rb += gridDim.x) {
+        const size_t row0 = rb * RB;
+        T acc[RB];
+        const V *arow[RB];
+#pragma unroll
+        for (int r = 0; r < RB; ++r) {
+            acc[r] = T(0);
+            const size_t row = (row0 + r < a.M) ? row0 + r : a.M - 1;  // clamp; result discarded
+            arow[r] = reinterpret_cast<const V *>(A + row * a.lda);
+        }
+        size_t c = threadIdx.x;
+        for (; c + (UNROLL - 1) * kGemvThreads < nvec; c += UNROLL * kGemvThreads) {
+            V av[RB][UNROLL], xv[UNROLL];
+#pragma unroll
+            for (int u = 0; u < UNROLL; ++u) xv[u] = __ldg(x + c + u * kGemvThreads);
+#pragma unroll
+            for (int r = 0; r < RB; ++r)
+#pragma unroll
+                for (int u = 0; u < UNROLL; ++u) av[r][u] = __ldcs(arow[r] + c + u * kGemvThreads);
+#pragma unroll
+            for (int u = 0; u < UNROLL; ++u)
+#pragma unroll
+                for (int r = 0; r < RB; ++r) acc[r] = dot_acc(acc[r], av[r][u], xv[u]);
+        }
+        for (; c < nvec; c += kGemvThreads) {
+            const V xv = __ldg(x + c);
+#pragma unroll
+            for (int r = 0; r < RB; ++r) acc[r] = dot_acc(acc[r], __ldcs(arow[r] + c), xv);
+        }
+#pragma unroll
+        for (int r = 0; r < RB; ++r) {
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], off);
+        }
+        if (lane == 0)
+#pragma unroll
+            for (int r = 0; r < RB; ++r) red[r][w] = acc[r];
+        __syncthreads();
+        if (threadIdx.x < RB) {
+            const int r = threadIdx.x;
+            T v = red[r][0];
+#pragma unroll
+            for (int ww = 1; ww < kGemvWarps; ++ww) v += red[r][ww];
+            const size_t row = row0 + r;
+            if (row < a.M) y[row] = epilogue<T>(a.gemv, alpha, beta, v, y + row);
+        }
+        __syncthreads();
     }
 }
 
@@ -327,6 +399,17 @@ static int matvec_launch(const gatlas_matvec_desc *d, const T *A, const T *x, T 
     const bool vec_ok = gemv_vec_ok<T>(d, A, x);
     const int sms = sm_count();
     if (!d->trans_a) {
+        constexpr int UNROLL = 4;
+        constexpr int VWV = 16 / sizeof(T);
+        if (vec_ok && d->n / VWV >= (size_t)UNROLL * kGemvThreads) {
+            // long rows: a CTA per RB rows (see gemv_rowblock_kernel)
+            constexpr int RB = 2;
+            const size_t nblocks = (d->m + RB - 1) / RB;
+            const size_t cap = (size_t)sms * 64 / (batch < 8 ? batch : 8);
+            dim3 g((unsigned)(nblocks < cap ? nblocks : cap), (unsigned)batch);
+            gemv_rowblock_kernel<T, VWV, RB, UNROLL><<<g, kGemvThreads, 0, stream>>>(a);
+            return check_launch("gemv_rowblock_kernel");
+        }
         constexpr int ROWS = 2;
         const size_t warps_needed = (d->m + ROWS - 1) / ROWS;
         size_t grid = (warps_needed + kGemvWarps - 1) / kGemvWarps;

@@ -10,8 +10,8 @@
 //    (evict-first) loads and stores, grid = SMs x 8 blocks of 256 threads.
 //  * image engine: persistent CTAs stream 16 KiB chunks of x and y into shared
 //    memory with 1-D bulk async copies (cp.async.bulk, TMA engine) through a
-//    4-stage mbarrier pipeline, compute in place, and write back with bulk
-//    shared->global copies.
+//    6-stage mbarrier pipeline (loads four chunks ahead), compute in place,
+//    and write back with bulk shared->global copies.
 // Both compute __fma_rn(alpha, x, y): bit-exact against a per-element fmaf.
 #include "../common.cuh"
 #include "../device_state.cuh"
@@ -73,7 +73,12 @@ __global__ void __launch_bounds__(kSaxpyThreads)
 // image engine: bulk-copy pipeline
 // ---------------------------------------------------------------------------
 constexpr int kBulkThreads = 256;
-constexpr int kBulkStages = 4;
+constexpr int kBulkStages = 6;
+// Loads run kBulkAhead chunks ahead, so the stage a new load reuses was last
+// stored from two chunks ago: the producer waits only for that older bulk
+// store to finish reading shared memory (wait_group.read 1), never for the
+// store just committed.
+constexpr int kBulkAhead = kBulkStages - 2;
 constexpr uint32_t kBulkChunkBytes = 16384;  // per operand per stage
 
 template <typename T>
@@ -118,16 +123,17 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
 
     size_t issued = 0;  // meaningful in thread 0 only
     if (threadIdx.x == 0)
-        for (; issued < (size_t)(kBulkStages - 1) && issued < mine; ++issued) issue(issued);
+        for (; issued < (size_t)kBulkAhead && issued < mine; ++issued) issue(issued);
 
     size_t i = 0;
     for (; i < mine; ++i) {
         const int s = (int)(i % kBulkStages);
-        if (threadIdx.x == 0 && i + kBulkStages - 1 < mine) {
-            // stage (i-1) % S is reused: its bulk store must have finished reading smem
-            bulk_wait_read<0>();
-            issue(i + kBulkStages - 1);
-            issued = i + kBulkStages;
+        if (threadIdx.x == 0 && i + kBulkAhead < mine) {
+            // stage (i - 2) % S is reused: the bulk store of chunk i - 2 (every
+            // committed group but the newest) must have finished reading smem
+            bulk_wait_read<1>();
+            issue(i + kBulkAhead);
+            issued = i + kBulkAhead + 1;
         }
         if (!mbar_wait_bounded(&full[s], (uint32_t)((i / kBulkStages) & 1), 1u << 22)) {
             report_fault(fault, kFaultSaxpyBulkWait);

@@ -47,7 +47,7 @@ def test_known_answer_c_equals_n(cuda, ta, M, N):
 
 @pytest.mark.parametrize("ta", [0, 1])
 @pytest.mark.parametrize("M,N", [(1, 1), (1, 37), (37, 1), (33, 65), (127, 129), (1000, 1001),
-                                 (2048, 3072), (4099, 257)])
+                                 (2048, 3072), (4099, 257), (301, 4096), (1001, 6000), (7, 10003), (3, 65536)])
 def test_tolerance_vs_f64(cuda, ta, M, N):
     A = oracle.uniform(M * N, seed=M * 7 + N)
     x = oracle.uniform(N, seed=N * 3 + 1)
