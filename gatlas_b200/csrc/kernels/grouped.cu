@@ -397,11 +397,30 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
             const TileRec *R = p.tiles + t;
             const int bn = R->bn, kt = R->kt;
             const int hw = bn >> 1;            // columns of this warp's half
-            const int nchunks = hw >> 5;       // 1, 2 or 4 chunks of 32 columns
             const int nseg = (kt + p.seg_kblocks - 1) / p.seg_kblocks;
+            // Accumulator fragments in the 16x256b layout: for row slab rs (TMEM
+            // lanes 16*rs .. 16*rs+15 of this warp's quarter) and column group
+            // cg (8 columns), acc[(rs*16 + cg)*4 + e] holds row
+            // 16*rs + lane/4 (e = 0, 1) or 16*rs + lane/4 + 8 (e = 2, 3), column
+            // 8*cg + 2*(lane%4) + (e & 1) of this warp's half of the tile.  Four
+            // neighbouring lanes then hold 32 contiguous bytes of one row of C,
+            // so each store request covers whole sectors of eight rows.
             float acc[128];
 #pragma unroll
             for (int j = 0; j < 128; ++j) acc[j] = 0.0f;
+            const int ngroups = hw >> 3;         // 8-column groups of this warp's half: 4, 8 or 16
+            {
+                // C is read by the epilogue (beta != 0): pull this warp's rows
+                // of it into L2 while the tile's MMAs run
+                const int r = quarter * 32 + lane;
+                if (R->gemm && R->beta != 0.0f && r < R->rows) {
+                    const int left = R->cols - half * hw;
+                    const int ncols = left < hw ? left : hw;
+                    const char *row = reinterpret_cast<const char *>(R->C + (int64_t)r * R->ldc + half * hw);
+                    for (int off = 0; off < ncols * 4; off += 128)
+                        asm volatile("prefetch.global.L2 [%0];" ::"l"(row + off));
+                }
+            }
             for (int sg = 0; sg < nseg; ++sg, ++seg) {
                 const int b = seg & 1;
                 if (!tc::wait_timed(&tfull[b], (uint32_t)(seg >> 1) & 1u, 2 * kWaitNs, &abort_flag)) {
@@ -413,13 +432,19 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
                 tc::fence_after_sync();
                 const uint32_t col_base = tmem + lane_base + (uint32_t)(b * 256 + half * hw);
 #pragma unroll
-                for (int c = 0; c < 8; ++c) {
-                    if (c < 2 * nchunks) {
-                        uint32_t r[16];
-                        tc::tmem_ld_32x32b_x16(col_base + (uint32_t)(c * 16), r);
-                        tc::tmem_ld_wait();
+                for (int rs = 0; rs < 2; ++rs) {
 #pragma unroll
-                        for (int j = 0; j < 16; ++j) acc[c * 16 + j] = __fadd_rn(acc[c * 16 + j], __uint_as_float(r[j]));
+                    for (int c = 0; c < 4; ++c) {   // 32 columns per load
+                        if (c * 4 < ngroups) {
+                            uint32_t r[16];
+                            tc::tmem_ld_16x256b_x4(col_base + ((uint32_t)(rs * 16) << 16) + (uint32_t)(c * 32), r);
+                            tc::tmem_ld_wait();
+#pragma unroll
+                            for (int j = 0; j < 16; ++j) {
+                                const int idx = (rs * 16 + c * 4) * 4 + j;
+                                acc[idx] = __fadd_rn(acc[idx], __uint_as_float(r[j]));
+                            }
+                        }
                     }
                 }
                 tc::fence_before_sync();
@@ -427,33 +452,53 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
                 if (lane == 0) mbar_arrive(&tempty[b]);
             }
             if (!ok || abort_flag) break;
-            const int r = quarter * 32 + lane;
-            if (r < R->rows) {
-                const int left = R->cols - half * hw;
-                const int ncols = left < hw ? left : hw;  // valid columns of this half
-                float *cp = R->C + (int64_t)r * R->ldc + half * hw;
-                const bool vec_ok = ((reinterpret_cast<uintptr_t>(cp) & 15) == 0);
-                const bool gemm = R->gemm != 0;
-                const float alpha = R->alpha, beta = gemm ? R->beta : 0.0f;
+            const int left = R->cols - half * hw;
+            const int ncols = left < hw ? left : hw;  // valid columns of this half
+            const bool gemm = R->gemm != 0;
+            const float alpha = R->alpha, beta = gemm ? R->beta : 0.0f;
+            const bool vec_ok = ((R->ldc & 1) == 0) && ((reinterpret_cast<uintptr_t>(R->C) & 7) == 0) &&
+                                ((half * hw) % 2 == 0);
+            const int cl = 2 * (lane & 3);
 #pragma unroll
-                for (int q = 0; q < 32; ++q) {
-                    const int jc = q * 4;
-                    if (jc >= ncols) break;
-                    float v[4];
-                    if (vec_ok && jc + 3 < ncols) {
-                        float4 c4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                        if (beta != 0.0f) c4 = *reinterpret_cast<const float4 *>(cp + jc);
-                        const float cv[4] = {c4.x, c4.y, c4.z, c4.w};
+            for (int rs = 0; rs < 2; ++rs) {
 #pragma unroll
-                        for (int e = 0; e < 4; ++e)
-                            v[e] = gemm ? __fmaf_rn(alpha, acc[jc + e], beta == 0.0f ? 0.0f : beta * cv[e]) : acc[jc + e];
-                        *reinterpret_cast<float4 *>(cp + jc) = make_float4(v[0], v[1], v[2], v[3]);
-                    } else {
+                for (int rr = 0; rr < 2; ++rr) {
+                    const int row = quarter * 32 + rs * 16 + (lane >> 2) + 8 * rr;
+                    if (row >= R->rows) continue;
+                    float *cp = R->C + (int64_t)row * R->ldc + half * hw;
+                    // four 8-column groups at a time: their loads of C
+                    // (beta != 0) are issued together, then their stores
 #pragma unroll
-                        for (int e = 0; e < 4; ++e) {
-                            if (jc + e < ncols) {
-                                const float bc = beta == 0.0f ? 0.0f : beta * cp[jc + e];
-                                cp[jc + e] = gemm ? __fmaf_rn(alpha, acc[jc + e], bc) : acc[jc + e];
+                    for (int g0 = 0; g0 < 16; g0 += 4) {
+                        if (g0 >= ngroups) break;
+                        float2 c2[4];
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const int col = (g0 + q) * 8 + cl;
+                            c2[q] = make_float2(0.0f, 0.0f);
+                            if (beta != 0.0f && vec_ok && col + 1 < ncols)
+                                c2[q] = *reinterpret_cast<const float2 *>(cp + col);
+                        }
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const int col = (g0 + q) * 8 + cl;
+                            const int idx = (rs * 16 + g0 + q) * 4 + 2 * rr;
+                            if (col >= ncols) continue;
+                            if (vec_ok && col + 1 < ncols) {
+                                float2 v;
+                                v.x = gemm ? __fmaf_rn(alpha, acc[idx], beta == 0.0f ? 0.0f : beta * c2[q].x)
+                                           : acc[idx];
+                                v.y = gemm ? __fmaf_rn(alpha, acc[idx + 1], beta == 0.0f ? 0.0f : beta * c2[q].y)
+                                           : acc[idx + 1];
+                                *reinterpret_cast<float2 *>(cp + col) = v;
+                            } else {
+#pragma unroll
+                                for (int e = 0; e < 2; ++e) {
+                                    if (col + e < ncols) {
+                                        const float bc = beta == 0.0f ? 0.0f : beta * cp[col + e];
+                                        cp[col + e] = gemm ? __fmaf_rn(alpha, acc[idx + e], bc) : acc[idx + e];
+                                    }
+                                }
                             }
                         }
                     }
