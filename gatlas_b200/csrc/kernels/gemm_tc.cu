@@ -23,9 +23,8 @@
 //     drain warps promote each segment into round-to-nearest FP32 registers
 //     and, at the end of a tile, apply C = fma(alpha, acc, beta*C) and store
 //     C through TMA while the next tile already runs.  FP8 E4M3 (per-block
-//     scales) runs the same persistent kernel on single CTAs, its segments
-//     planned per tile by fp8_plan_kernel; FP8 pairs (opt-in) run one tile
-//     per cluster (tc_gemm_pair_kernel).
+//     scales) runs the same persistent kernel, on single CTAs or pairs, its
+//     segments planned per tile by fp8_plan_kernel.
 // Every mbarrier wait is bounded in wall time; a timeout sets the device
 // fault word, stops the pipeline, drains the copies in flight and frees TMEM.
 #include <cuda.h>
@@ -88,8 +87,19 @@ constexpr int kThreads2 = 32 * (2 + kDrainWarps);
 constexpr uint32_t kTmemCols2 = 2 * BN;  // two accumulator buffers
 
 // ---------------------------------------------------------------------------
-// CTA-pair contraction (cta_group::2): one 256 x 256 tile per cluster of two
-// ---------------------------------------------------------------------------
+// Persistent contraction: one CTA (or CTA pair) per SM walks
+// the tiles t = unit, unit + units, ... in the grouped raster order.  The
+// ring, the MMA issue and the TMEM double buffer run on across tile
+// boundaries, so one tile's last promotions and its C stores overlap the
+// next tile's loads and MMAs; each drain warp stages its 32 x 128 block of C
+// through a 32 x 32 shared-memory tile (128-byte swizzle) and a TMA store,
+// which also clips the tile at M and N.
+// FP8 (MODE 3): segments follow the per-tile plan written by fp8_plan_kernel
+// (runs of equally scaled 128-deep blocks); the MMA issuer reads its
+// segment-start bits a 32-block word ahead, the drain scales each segment as
+// it promotes it (on a pair, with the products of its own CTA's rows).
+//
+// PAIR (cta_group::2, one 256 x 256 tile per cluster of two CTAs):
 // Each CTA streams 128 rows of A and its 128-row half of B per K slice
 // (instead of 128 + 256 rows for a 128 x 256 tile), so the operand bytes
 // moved from L2 per FLOP fall by a third and the ring gets deeper for the
@@ -104,319 +114,6 @@ constexpr uint32_t kTmemCols2 = 2 * BN;  // two accumulator buffers
 // Every wait is bounded; after an abort each CTA lets in-flight copies land
 // before the closing cluster barrier, so neither CTA leaves while the pair's
 // MMAs or copies can still touch its shared memory.
-template <int MODE>
-__global__ void __launch_bounds__(kThreads2, 1)
-    tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap ta0, const __grid_constant__ CUtensorMap ta1,
-                        const __grid_constant__ CUtensorMap ta2, const __grid_constant__ CUtensorMap tb0,
-                        const __grid_constant__ CUtensorMap tb1, const __grid_constant__ CUtensorMap tb2,
-                        Params p) {
-    using L = PairLayout<MODE>;
-    using MD = Mode<MODE>;
-    constexpr int S = L::STAGES;
-    constexpr int BK = L::BK;
-    extern __shared__ uint8_t smem_raw[];
-    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    __shared__ __align__(8) uint64_t full[S], empty[S], tfull[2], tempty[2], mma_done;
-    __shared__ uint32_t tmem_base;
-    __shared__ volatile int abort_flag;
-    __shared__ int kb_issued, kb_consumed, mma_aborted, fp8_nseg;
-
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t rank = tc::cluster_ctarank();
-    const bool leader = rank == 0;
-    int tile_m, tile_n;  // in pair tiles (256 x 256)
-    {
-        const int tiles_n = (int)((p.N + L::PN - 1) / L::PN), tiles_m = (int)((p.M + L::PM - 1) / L::PM);
-        const int bid = (int)(blockIdx.x >> 1);
-        const int per_group = kGroupM * tiles_n;
-        const int first_m = (bid / per_group) * kGroupM;
-        const int gm = min(tiles_m - first_m, kGroupM);
-        const int r = bid % per_group;
-        tile_m = first_m + r % gm;
-        tile_n = r / gm;
-    }
-    const int m0 = tile_m * L::PM + (int)rank * 128;  // this CTA's rows of A and C
-    const int n0 = tile_n * L::PN;                    // the pair's columns
-    const int nb = n0 + (int)rank * 128;              // this CTA's half of B
-    const int z = blockIdx.z;
-    const CUtensorMap *tA[3] = {&ta0, &ta1, &ta2};
-    const CUtensorMap *tB[3] = {&tb0, &tb1, &tb2};
-
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < S; ++s) {
-            mbar_init(&full[s], 1);
-            mbar_init(&empty[s], 1);
-        }
-        for (int b = 0; b < 2; ++b) {
-            mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], 2 * kDrainWarps);
-        }
-        mbar_init(&mma_done, 1);
-        fence_mbarrier_init();
-        abort_flag = 0;
-        kb_issued = kb_consumed = 0;
-        mma_aborted = 0;
-        for (int i = 0; i < MD::NP; ++i) {
-            prefetch_tmap(tA[i]);
-            prefetch_tmap(tB[i]);
-        }
-    }
-    if (warp == 0) {
-        tc::tmem_alloc_pair(&tmem_base, kTmemCols2);
-        tc::tmem_relinquish_pair();
-    }
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::cluster_sync();  // both CTAs' barriers exist before any signal crosses the pair
-    tc::fence_after_sync();
-    const uint32_t tmem = tmem_base;
-
-    // Segment plan, identical in both CTAs (the leader's MMA serves both).
-    // FP8: a run of at most seg_kblocks blocks whose four scale products (the
-    // pair's two row blocks x two column halves) are all unchanged; each CTA
-    // keeps the segment scales of its own row block.
-    float *seg_q0 = nullptr, *seg_q1 = nullptr;
-    uint8_t *seg_flag = nullptr;
-    int nseg = (p.kblocks + p.seg_kblocks - 1) / p.seg_kblocks;
-    if constexpr (MD::SCALED) {
-        seg_q0 = reinterpret_cast<float *>(smem + S * L::STAGE_BYTES);
-        seg_q1 = seg_q0 + kMaxFp8Blocks;
-        seg_flag = reinterpret_cast<uint8_t *>(seg_q1 + kMaxFp8Blocks);
-        const float *sa[2], *sb[2];
-        for (int i = 0; i < 2; ++i) {
-            const int mb = tile_m * 2 + i, nbk = tile_n * 2 + i;
-            sa[i] = mb < p.nblocks_m ? p.scale_a + z * p.scale_a_stride + (int64_t)mb * p.kblocks : nullptr;
-            sb[i] = nbk < p.nblocks_n ? p.scale_b + z * p.scale_b_stride + (int64_t)nbk * p.kblocks : nullptr;
-        }
-        // per block: change flag of the four products, and this row block's two products
-        for (int kb = threadIdx.x; kb < p.kblocks; kb += blockDim.x) {
-            float q[2][2];
-            for (int i = 0; i < 2; ++i)
-                for (int h = 0; h < 2; ++h) q[i][h] = (sa[i] && sb[h]) ? __fmul_rn(sa[i][kb], sb[h][kb]) : 0.0f;
-            bool change = kb == 0;
-            if (kb > 0)
-                for (int i = 0; i < 2; ++i)
-                    for (int h = 0; h < 2; ++h) {
-                        const float prev = (sa[i] && sb[h]) ? __fmul_rn(sa[i][kb - 1], sb[h][kb - 1]) : 0.0f;
-                        change = change || prev != q[i][h];
-                    }
-            seg_q0[kb] = q[rank][0];
-            seg_q1[kb] = q[rank][1];
-            seg_flag[kb] = change ? 1 : 0;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int s = -1, run = 0;
-            for (int kb = 0; kb < p.kblocks; ++kb) {
-                const bool start = seg_flag[kb] != 0 || run == p.seg_kblocks;
-                if (start) {
-                    ++s;
-                    run = 0;
-                    seg_q0[s] = seg_q0[kb];  // s <= kb: compacted in place
-                    seg_q1[s] = seg_q1[kb];
-                }
-                seg_flag[kb] = start ? 1 : 0;
-                ++run;
-            }
-            fp8_nseg = s + 1;
-        }
-        __syncthreads();
-        nseg = fp8_nseg;
-    }
-
-    auto a_tile = [&](int s, int piece) { return smem + s * L::STAGE_BYTES + piece * L::A_TILE; };
-    auto b_tile = [&](int s, int piece) { return smem + s * L::STAGE_BYTES + MD::NP * L::A_TILE + piece * L::B_TILE; };
-    const uint32_t full_leader = tc::mapa_shared(smem_u32(&full[0]), 0);
-    const uint32_t tempty_leader = tc::mapa_shared(smem_u32(&tempty[0]), 0);
-
-    if (warp == 0) {
-        if (lane == 0) {
-            // ---- TMA producer (both CTAs): completion counts on the leader's full[s] ----
-            int kb = 0;
-            for (; kb < p.kblocks; ++kb) {
-                const int s = kb % S;
-                const uint32_t ph = (uint32_t)(kb / S) & 1u;
-                if (!tc::wait_timed_cluster(&empty[s], ph ^ 1u, kWaitNs, &abort_flag)) {
-                    if (!abort_flag) report_fault(p.fault, kFaultTcProducerWait);
-                    abort_flag = 1;
-                    break;
-                }
-                if (leader) mbar_arrive_expect_tx(&full[s], 2 * L::STAGE_BYTES);
-                const uint32_t bar = full_leader + (uint32_t)(s * sizeof(uint64_t));
-                for (int i = 0; i < MD::NP; ++i) {
-                    tc::tma_load_3d_pair(a_tile(s, i), tA[i], kb * BK, m0, z, bar);
-                    tc::tma_load_3d_pair(b_tile(s, i), tB[i], kb * BK, nb, z, bar);
-                }
-            }
-            kb_issued = kb;
-        }
-        __syncwarp();
-    } else if (warp == 1) {
-        if (lane == 0 && leader) {
-            // ---- MMA issuer (leader only) ----
-            constexpr uint32_t idesc = L::IDESC;
-            const uint32_t empty_self = tc::mapa_shared(smem_u32(&empty[0]), 0);
-            const uint32_t empty_peer = tc::mapa_shared(smem_u32(&empty[0]), 1);
-            const uint32_t tfull_self = tc::mapa_shared(smem_u32(&tfull[0]), 0);
-            const uint32_t tfull_peer = tc::mapa_shared(smem_u32(&tfull[0]), 1);
-            int kb = 0, seg = -1;
-            bool stop = false;
-            for (; kb < p.kblocks; ++kb) {
-                bool seg_first, seg_last;
-                if constexpr (MD::SCALED) {
-                    seg_first = seg_flag[kb] != 0;
-                    seg_last = kb == p.kblocks - 1 || seg_flag[kb + 1] != 0;
-                } else {
-                    seg_first = (kb % p.seg_kblocks) == 0;
-                    seg_last = (kb % p.seg_kblocks) == p.seg_kblocks - 1 || kb == p.kblocks - 1;
-                }
-                if (seg_first) ++seg;
-                const int b = seg & 1;
-                if (seg_first) {
-                    // both CTAs' drains of this buffer's previous segment are done
-                    if (!tc::wait_timed_cluster(&tempty[b], ((uint32_t)(seg >> 1) & 1u) ^ 1u, kWaitNs, &abort_flag)) {
-                        if (!abort_flag) report_fault(p.fault, kFaultTcMmaWait);
-                        abort_flag = 1;
-                        stop = true;
-                        break;
-                    }
-                    tc::fence_after_sync();
-                }
-                const int s = kb % S;
-                if (!tc::wait_timed_cluster(&full[s], (uint32_t)(kb / S) & 1u, kWaitNs, &abort_flag)) {
-                    if (!abort_flag) report_fault(p.fault, kFaultTcMmaWait);
-                    abort_flag = 1;
-                    stop = true;
-                    break;
-                }
-                tc::fence_after_sync();
-                const uint32_t d = tmem + (uint32_t)(b * 256);
-#pragma unroll
-                for (int kk = 0; kk < L::KSTEPS; ++kk) {
-#pragma unroll
-                    for (int j = 0; j < MD::NPROD; ++j) {
-                        const uint32_t a_addr = smem_u32(a_tile(s, MD::pa(j))) + kk * 32;
-                        const uint32_t b_addr = smem_u32(b_tile(s, MD::pb(j))) + kk * 32;
-                        const uint64_t ad = tc::smem_desc_kmajor(a_addr, L::SBO, L::SWIZZLE);
-                        const uint64_t bd = tc::smem_desc_kmajor(b_addr, L::SBO, L::SWIZZLE);
-                        const uint32_t accum = (seg_first && kk == 0 && j == 0) ? 0u : 1u;
-                        if constexpr (MD::SCALED) tc::mma_f8_pair(d, ad, bd, idesc, accum);
-                        else tc::mma_bf16_pair(d, ad, bd, idesc, accum);
-                    }
-                }
-                const uint32_t so = (uint32_t)(s * sizeof(uint64_t)), bo = (uint32_t)(b * sizeof(uint64_t));
-                tc::commit_pair_to(empty_self + so);
-                tc::commit_pair_to(empty_peer + so);
-                if (seg_last) {
-                    tc::commit_pair_to(tfull_self + bo);
-                    tc::commit_pair_to(tfull_peer + bo);
-                }
-            }
-            kb_consumed = kb;
-            if (stop) {
-                mma_aborted = 1;
-                tc::commit_pair_to(tc::mapa_shared(smem_u32(&mma_done), 0));
-            }
-        }
-        __syncwarp();
-    } else {
-        // ---- drain (both CTAs): promote each segment into FP32 registers ----
-        const int quarter = warp & 3, half = (warp - 2) >> 2;
-        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
-        float acc[128];
-#pragma unroll
-        for (int j = 0; j < 128; ++j) acc[j] = 0.0f;
-        bool ok = true;
-        for (int seg = 0; seg < nseg; ++seg) {
-            const int b = seg & 1;
-            float scale = 1.0f;
-            if constexpr (MD::SCALED) scale = half ? seg_q1[seg] : seg_q0[seg];
-            if (!tc::wait_timed_cluster(&tfull[b], (uint32_t)(seg >> 1) & 1u, 2 * kWaitNs, &abort_flag)) {
-                if (!abort_flag) report_fault(p.fault, kFaultTcEpilogueWait);
-                abort_flag = 1;
-                ok = false;
-                break;
-            }
-            tc::fence_after_sync();
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                uint32_t r[32];
-                tc::tmem_ld_32x32b_x32(tmem + lane_base + (uint32_t)(b * 256 + half * 128 + c * 32), r);
-                tc::tmem_ld_wait();
-#pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    if constexpr (MD::SCALED)
-                        acc[c * 32 + j] = __fmaf_rn(__uint_as_float(r[j]), scale, acc[c * 32 + j]);
-                    else
-                        acc[c * 32 + j] = __fadd_rn(acc[c * 32 + j], __uint_as_float(r[j]));
-                }
-            }
-            tc::fence_before_sync();
-            __syncwarp();
-            if (lane == 0) {
-                if (leader) mbar_arrive(&tempty[b]);
-                else tc::mbar_arrive_remote(tempty_leader + (uint32_t)(b * sizeof(uint64_t)));
-            }
-        }
-        if (ok && !abort_flag) {
-            const int64_t row = (int64_t)m0 + quarter * 32 + lane;
-            float *crow = p.C + (int64_t)z * p.stride_c + row * p.ldc;
-            const bool vec_ok = (p.ldc % 4 == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0) &&
-                                (p.stride_c % 4 == 0);
-            if (row < p.M) {
-                const int64_t col0 = (int64_t)n0 + half * 128;
-#pragma unroll
-                for (int j = 0; j < 128; j += 4) {
-                    float v[4];
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const int64_t col = col0 + j + e;
-                        if (p.gemm) {
-                            const float bc = (p.beta == 0.0f || col >= p.N) ? 0.0f : p.beta * crow[col];
-                            v[e] = __fmaf_rn(p.alpha, acc[j + e], bc);
-                        } else {
-                            v[e] = acc[j + e];
-                        }
-                    }
-                    if (vec_ok && col0 + j + 3 < p.N) {
-                        *reinterpret_cast<float4 *>(crow + col0 + j) = make_float4(v[0], v[1], v[2], v[3]);
-                    } else {
-#pragma unroll
-                        for (int e = 0; e < 4; ++e)
-                            if (col0 + j + e < p.N) crow[col0 + j + e] = v[e];
-                    }
-                }
-            }
-        }
-    }
-    tc::fence_before_sync();
-    __syncthreads();
-    if (threadIdx.x == 0 && abort_flag) {
-        // This CTA's copies complete on the leader's barrier, so they cannot be
-        // awaited here: give them time to land (they take microseconds).  The
-        // leader also waits for the MMAs issued before its abort.
-        const uint64_t t0 = tc::globaltimer();
-        while (tc::globaltimer() - t0 < 20000000ull) {
-        }
-        if (leader && mma_aborted) tc::wait_timed(&mma_done, 0, kWaitNs, nullptr);
-    }
-    __syncthreads();
-    tc::cluster_sync();  // neither CTA leaves while the pair can still touch its memory
-    if (warp == 0) tc::tmem_dealloc_pair(tmem, kTmemCols2);
-}
-
-// ---------------------------------------------------------------------------
-// Persistent contraction: one CTA (or CTA pair) per SM walks
-// the tiles t = unit, unit + units, ... in the grouped raster order.  The
-// ring, the MMA issue and the TMEM double buffer run on across tile
-// boundaries, so one tile's last promotions and its C stores overlap the
-// next tile's loads and MMAs; each drain warp stages its 32 x 128 block of C
-// through a 32 x 32 shared-memory tile (128-byte swizzle) and a TMA store,
-// which also clips the tile at M and N.  PAIR as in tc_gemm_pair_kernel.
-// FP8 (MODE 3, single CTAs): segments follow the per-tile plan written by
-// fp8_plan_kernel (runs of equally scaled 128-deep blocks); the MMA issuer
-// reads its segment-start bits a 32-block word ahead, the drain scales each
-// segment as it promotes it.
 // ---------------------------------------------------------------------------
 template <int MODE, bool PAIR>
 __global__ void __launch_bounds__(kThreads2, 1)
@@ -605,7 +302,8 @@ __global__ void __launch_bounds__(kThreads2, 1)
                             const uint64_t ad = tc::smem_desc_kmajor(a_addr, L::SBO, L::SWIZZLE);
                             const uint64_t bd = tc::smem_desc_kmajor(b_addr, L::SBO, L::SWIZZLE);
                             const uint32_t accum = (seg_first && kk == 0 && j == 0) ? 0u : 1u;
-                            if constexpr (MD::SCALED) tc::mma_f8(d, ad, bd, idesc, accum);
+                            if constexpr (MD::SCALED && PAIR) tc::mma_f8_pair(d, ad, bd, idesc, accum);
+                            else if constexpr (MD::SCALED) tc::mma_f8(d, ad, bd, idesc, accum);
                             else if constexpr (PAIR) tc::mma_bf16_pair(d, ad, bd, idesc, accum);
                             else tc::mma_bf16(d, ad, bd, idesc, accum);
                         }
@@ -656,7 +354,8 @@ __global__ void __launch_bounds__(kThreads2, 1)
             if constexpr (MD::SCALED) {
                 const int64_t pidx = ((int64_t)z * p.tiles_m + tm) * p.tiles_n + tn;
                 tile_nseg = __ldg(p.plan_nseg + pidx);
-                tile_q = p.plan_q + pidx * p.kblocks;
+                // a pair's plan holds the products of both CTAs' rows per segment
+                tile_q = p.plan_q + pidx * p.kblocks * (PAIR ? 2 : 1) + (PAIR ? rank : 0);
             }
             float acc[BN / 2];
 #pragma unroll
@@ -666,7 +365,7 @@ __global__ void __launch_bounds__(kThreads2, 1)
                 const int b = seg & 1;
                 float scale = 1.0f;
                 if constexpr (MD::SCALED) {
-                    const float2 q = __ldg(tile_q + g);  // this half's scale block product
+                    const float2 q = __ldg(tile_q + (PAIR ? 2 * g : g));  // this half's scale block product
                     scale = half ? q.y : q.x;
                 }
                 if (!wait(&tfull[b], (uint32_t)(seg >> 1) & 1u, 2 * kWaitNs)) {
@@ -1294,12 +993,15 @@ static bool make_plan(const gatlas_matmul_desc *d, const Geometry &g, Plan *pl) 
         pl->kblocks = (int64_t)((K + kQBlock - 1) / kQBlock);
         pl->sa_bytes = round_up((size_t)g.batch * pl->mblocks * pl->kblocks * 4, 1024);
         pl->sb_bytes = round_up((size_t)g.batch * pl->nblocks * pl->kblocks * 4, 1024);
-        // tiles of 128 x 256: per tile a segment count, one bit per block, a
-        // scale pair per possible segment
-        const size_t tiles = (size_t)((g.M + BM - 1) / BM) * (size_t)((g.N + BN - 1) / BN) * (size_t)g.batch;
+        // per tile a segment count, one bit per block and the scale products
+        // of every possible segment: tiles of 128 x 256 (single CTAs, two
+        // products) or 256 x 256 (CTA pairs, four); sized for either
+        const size_t tn = (size_t)((g.N + BN - 1) / BN) * (size_t)g.batch;
+        const size_t tiles = (size_t)((g.M + BM - 1) / BM) * tn;
+        const size_t pair_tiles = (size_t)((g.M + 2 * BM - 1) / (2 * BM)) * tn;
         pl->plan_nseg_bytes = round_up(tiles * 4, 256);
         pl->plan_bits_bytes = round_up(tiles * (size_t)((pl->kblocks + 31) / 32) * 4, 256);
-        pl->plan_q_bytes = round_up(tiles * (size_t)pl->kblocks * 8, 1024);
+        pl->plan_q_bytes = round_up(std::max(tiles, 2 * pair_tiles) * (size_t)pl->kblocks * 8, 1024);
     }
     pl->total = pl->np * (pl->a_piece_bytes + pl->b_piece_bytes) + pl->sa_bytes + pl->sb_bytes +
                 pl->plan_nseg_bytes + pl->plan_bits_bytes + pl->plan_q_bytes;
@@ -1398,44 +1100,57 @@ static int g_tc_pair = 1;
 // Rows of C per raster group of the persistent kernels (multiple of 128).
 static int g_tc_group_rows = kGroupM * 128;
 
-// FP8 segment plan, one thread per 128 x 256 tile: a run of at most
-// seg_kblocks 128-deep blocks whose scale products sa * sb are equal for both
-// column halves of the tile accumulates in TMEM and is promoted, scaled once
-// (exact: the scales are powers of two).  Writes the tile's segment count,
-// its segment-start bits and each segment's two scale products.
+// FP8 segment plan, one thread per tile: a run of at most seg_kblocks
+// 128-deep blocks whose scale products sa * sb are equal for every 128 x 128
+// block of the tile accumulates in TMEM and is promoted, scaled once (exact:
+// the scales are powers of two).  Writes the tile's segment count, its
+// segment-start bits and each segment's scale products.  Single CTAs
+// (pair == 0) have 128 x 256 tiles: one A block, two column halves, products
+// (a b0, a b1) per segment.  CTA pairs (pair == 1) have 256 x 256 tiles: the
+// MMAs of both CTAs share their segments, so a run ends where any of the four
+// products changes; per segment the plan holds (a0 b0, a0 b1) for the
+// leader's rows and (a1 b0, a1 b1) for the peer's.
 __global__ void __launch_bounds__(128)
     fp8_plan_kernel(const float *scale_a, const float *scale_b, int64_t sa_stride, int64_t sb_stride, int tiles_m,
-                    int tiles_n, int batch, int kblocks, int nblocks_n, int seg_kblocks, int words, int *nseg,
-                    uint32_t *bits, float2 *q) {
+                    int tiles_n, int batch, int kblocks, int nblocks_m, int nblocks_n, int seg_kblocks, int words,
+                    int pair, int *nseg, uint32_t *bits, float2 *q) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (int64_t)tiles_m * tiles_n * batch) return;
     const int tn = (int)(idx % tiles_n);
     const int64_t rest = idx / tiles_n;
     const int tm = (int)(rest % tiles_m);
     const int64_t z = rest / tiles_m;
-    const float *sa = scale_a + z * sa_stride + (int64_t)tm * kblocks;
+    const int ma0 = pair ? 2 * tm : tm, ma1 = 2 * tm + 1;
+    const float *sa0 = scale_a + z * sa_stride + (int64_t)ma0 * kblocks;
+    const float *sa1 = pair && ma1 < nblocks_m ? scale_a + z * sa_stride + (int64_t)ma1 * kblocks : nullptr;
     const int nb0 = 2 * tn, nb1 = 2 * tn + 1;
     const float *sb0 = nb0 < nblocks_n ? scale_b + z * sb_stride + (int64_t)nb0 * kblocks : nullptr;
     const float *sb1 = nb1 < nblocks_n ? scale_b + z * sb_stride + (int64_t)nb1 * kblocks : nullptr;
     uint32_t *wb = bits + idx * words;
-    float2 *qt = q + idx * kblocks;
+    float2 *qt = q + idx * kblocks * (pair ? 2 : 1);
     int s = -1, run = 0;
-    float prev0 = 0.0f, prev1 = 0.0f;
+    float prev[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     uint32_t w = 0;
     for (int kb = 0; kb < kblocks; ++kb) {
-        const float a = sa[kb];
-        const float q0 = sb0 ? __fmul_rn(a, sb0[kb]) : 0.0f;
-        const float q1 = sb1 ? __fmul_rn(a, sb1[kb]) : 0.0f;
-        const bool start = kb == 0 || run == seg_kblocks || q0 != prev0 || q1 != prev1;
+        const float a0 = sa0[kb], a1 = sa1 ? sa1[kb] : 0.0f;
+        const float b0 = sb0 ? sb0[kb] : 0.0f, b1 = sb1 ? sb1[kb] : 0.0f;
+        const float cur[4] = {sb0 ? __fmul_rn(a0, b0) : 0.0f, sb1 ? __fmul_rn(a0, b1) : 0.0f,
+                              sa1 && sb0 ? __fmul_rn(a1, b0) : 0.0f, sa1 && sb1 ? __fmul_rn(a1, b1) : 0.0f};
+        bool start = kb == 0 || run == seg_kblocks;
+        for (int i = 0; i < 4; ++i) start = start || cur[i] != prev[i];
         if (start) {
             ++s;
             run = 0;
-            qt[s] = make_float2(q0, q1);
+            if (pair) {
+                qt[2 * s] = make_float2(cur[0], cur[1]);
+                qt[2 * s + 1] = make_float2(cur[2], cur[3]);
+            } else {
+                qt[s] = make_float2(cur[0], cur[1]);
+            }
             w |= 1u << (kb & 31);
         }
         ++run;
-        prev0 = q0;
-        prev1 = q1;
+        for (int i = 0; i < 4; ++i) prev[i] = cur[i];
         if ((kb & 31) == 31 || kb == kblocks - 1) {
             wb[kb >> 5] = w;
             w = 0;
@@ -1598,46 +1313,26 @@ static int launch_tc(const Geometry &g, const Plan &pl, const WsPtrs &w, float *
         return pair ? launch_persistent<MODE, true>(ta, tb, g, p, stream)
                     : launch_persistent<MODE, false>(ta, tb, g, p, stream);
     } else {
-    if (pair) {
-        using PL = PairLayout<MODE>;
-        const int smem = (int)PL::SMEM_BYTES;
-        cudaError_t e =
-            cudaFuncSetAttribute(tc_gemm_pair_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "tc pair smem attribute: %s", cudaGetErrorString(e));
-        const int64_t pairs = ((g.M + PL::PM - 1) / PL::PM) * ((g.N + PL::PN - 1) / PL::PN);
-        if (2 * pairs > 0x7fffffff) return set_error(GATLAS_ERR_INVALID, "matmul: too many tensor-core tiles");
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)(2 * pairs), 1, (unsigned)g.batch);
-        cfg.blockDim = dim3(kThreads2, 1, 1);
-        cfg.dynamicSmemBytes = (size_t)smem;
-        cfg.stream = stream;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = 2;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        e = cudaLaunchKernelEx(&cfg, tc_gemm_pair_kernel<MODE>, ta[0], ta[1], ta[2], tb[0], tb[1], tb[2], p);
-        if (e != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "tc_gemm_pair_kernel: %s", cudaGetErrorString(e));
-        return check_launch("tc_gemm_pair_kernel");
-    }
-    // single CTAs: plan every tile's segments, then the persistent kernel
-    const int64_t tiles_m = (g.M + BM - 1) / BM, tiles_n = (g.N + BN - 1) / BN;
-    const int64_t tiles = tiles_m * tiles_n * g.batch;
-    if (tiles > 0) {
-        const int words = (int)((p.kblocks + 31) / 32);
-        fp8_plan_kernel<<<(unsigned)((tiles + 127) / 128), 128, 0, stream>>>(
-            w.sa, w.sb, p.scale_a_stride, p.scale_b_stride, (int)tiles_m, (int)tiles_n, (int)g.batch, p.kblocks,
-            p.nblocks_n, p.seg_kblocks, words, w.plan_nseg, w.plan_bits, w.plan_q);
-        int rc = check_launch("fp8_plan_kernel");
-        if (rc) return rc;
-        p.plan_nseg = w.plan_nseg;
-        p.plan_bits = w.plan_bits;
-        p.plan_q = w.plan_q;
-        p.plan_words = words;
-    }
-    return launch_persistent<MODE, false>(ta, tb, g, p, stream);
+        // plan every tile's segments (256 x 256 tiles on CTA pairs, 128 x 256
+        // on single CTAs), then the persistent kernel
+        const int64_t tm_rows = pair ? 2 * BM : BM;
+        const int64_t tiles_m = (g.M + tm_rows - 1) / tm_rows, tiles_n = (g.N + BN - 1) / BN;
+        const int64_t tiles = tiles_m * tiles_n * g.batch;
+        if (tiles > 0) {
+            const int words = (int)((p.kblocks + 31) / 32);
+            fp8_plan_kernel<<<(unsigned)((tiles + 127) / 128), 128, 0, stream>>>(
+                w.sa, w.sb, p.scale_a_stride, p.scale_b_stride, (int)tiles_m, (int)tiles_n, (int)g.batch,
+                p.kblocks, p.nblocks_m, p.nblocks_n, p.seg_kblocks, words, pair ? 1 : 0, w.plan_nseg, w.plan_bits,
+                w.plan_q);
+            int rc = check_launch("fp8_plan_kernel");
+            if (rc) return rc;
+            p.plan_nseg = w.plan_nseg;
+            p.plan_bits = w.plan_bits;
+            p.plan_q = w.plan_q;
+            p.plan_words = words;
+        }
+        return pair ? launch_persistent<MODE, true>(ta, tb, g, p, stream)
+                    : launch_persistent<MODE, false>(ta, tb, g, p, stream);
     }
 }
 

@@ -97,31 +97,6 @@ struct Layout {
     static constexpr uint32_t IDESC = MD::SCALED ? tc::idesc_e4m3_f32(BM, BN) : tc::idesc_bf16_f32(BM, BN);
 };
 
-// CTA-pair layout (cta_group::2): one 256 x 256 tile per pair of CTAs.  Each
-// CTA stages its 128 rows of A and its 128-row half of B per K slice, and
-// holds its 128 rows of the accumulator in its own TMEM.
-template <int MODE>
-struct PairLayout {
-    using L1 = Layout<MODE>;
-    using MD = Mode<MODE>;
-    static constexpr int NP = MD::NP;
-    static constexpr int BK = L1::BK;
-    static constexpr uint32_t ROW_BYTES = L1::ROW_BYTES;
-    static constexpr uint32_t SWIZZLE = L1::SWIZZLE;
-    static constexpr uint32_t SBO = L1::SBO;
-    static constexpr int KSTEPS = L1::KSTEPS;
-    static constexpr int PM = 256, PN = 256;                 // pair tile
-    static constexpr uint32_t A_TILE = 128 * ROW_BYTES;      // this CTA's rows of A
-    static constexpr uint32_t B_TILE = 128 * ROW_BYTES;      // this CTA's half of B
-    static constexpr uint32_t STAGE_BYTES = NP * (A_TILE + B_TILE);
-    static constexpr uint32_t PLAN_BYTES = L1::PLAN_BYTES;
-    static constexpr uint32_t BUDGET = 226 * 1024;          // dynamic shared memory per CTA
-    static constexpr int STAGES = (int)((BUDGET - PLAN_BYTES - 1024) / STAGE_BYTES);
-    static constexpr uint32_t SMEM_BYTES = STAGES * STAGE_BYTES + PLAN_BYTES + 1024;
-    static constexpr uint32_t IDESC = MD::SCALED ? tc::idesc_e4m3_f32(PM, PN) : tc::idesc_bf16_f32(PM, PN);
-    static_assert(STAGES >= 3, "pair pipeline depth");
-};
-
 // Persistent layout: the ring, then one 32 x 32 FP32 staging
 // tile per drain warp for the TMA-store epilogue, which runs while the ring
 // already feeds the next tile.  PAIR: a 256 x 256 tile per cluster of two
@@ -147,7 +122,6 @@ struct PersistentLayout {
     static constexpr uint32_t EPI_OFFSET = STAGES * STAGE_BYTES;
     static constexpr uint32_t SMEM_BYTES = EPI_OFFSET + kEpiBytes + 1024;  // + alignment slack
     static constexpr uint32_t IDESC = MD::SCALED ? tc::idesc_e4m3_f32(TM, 256) : tc::idesc_bf16_f32(TM, 256);
-    static_assert(!(MD::SCALED && PAIR), "persistent FP8 runs on single CTAs");
     static_assert(STAGES >= 2, "tensor-core pipeline depth");
 };
 
