@@ -91,14 +91,16 @@ struct Tile {
     static_assert(TB || BN % VL == 0, "vector width must divide the B tile columns");
 };
 
-// FP32 points are capped at 128 registers so that 512 threads fit per SM.
-template <typename T, int NT>
+// FP32 points with micro-tiles of at most 64 elements are capped at 128
+// registers so that 512 threads fit per SM; larger micro-tiles take up to 255
+// registers at one CTA per SM, with the ILP of their accumulators instead.
+template <typename T, int NT, int MICRO>
 constexpr int min_blocks() {
-    return (sizeof(T) == 4 && NT <= 512) ? 512 / NT : 1;
+    return (sizeof(T) == 4 && NT <= 512 && MICRO <= 64) ? 512 / NT : 1;
 }
 
 template <typename T, bool TA, bool TB, int GH, int GW, int BH, int BW, int VL, int BK>
-__global__ void __launch_bounds__(GH *GW, min_blocks<T, GH * GW>())
+__global__ void __launch_bounds__(GH *GW, min_blocks<T, GH * GW, BH * BW>())
     gemm_simt_kernel(GemmArgs<T> a) {
     using TT = Tile<T, TA, TB, GH, GW, BH, BW, VL, BK>;
     constexpr int NT = TT::NT, BM = TT::BM, BN = TT::BN;
