@@ -969,7 +969,8 @@ def run_tc_sweep(args) -> None:
     sampled through NVML.  One JSON line per point; cycles = ms x median MHz.
     Pair settings (gatlas_set_option "tc_pair"): 1 the default choice (CTA
     pairs for split3/split6, 256 x 256 single-CTA tiles for BF16), 0 single
-    CTAs on 128 x 256 tiles, 2 CTA pairs."""
+    CTAs on 128 x 256 tiles, 2 CTA pairs.  L2 hints ("tc_l2_hint"): 0 none,
+    1 A evict-last and B evict-first, 2 the opposite."""
     import time
 
     import torch
@@ -979,6 +980,7 @@ def run_tc_sweep(args) -> None:
     torch.cuda.set_device(dev)
     engines = args.sweep_engines.split(",")
     rows_list = [int(x) for x in args.sweep_group_rows.split(",")]
+    hints = [int(x) for x in args.sweep_l2_hints.split(",")]
     for M in (int(x) for x in args.tc_sweep.split(",")):
         A = torch.empty(M * M, device=dev)
         B = torch.empty(M * M, device=dev)
@@ -991,8 +993,9 @@ def run_tc_sweep(args) -> None:
                 ws = torch.empty(g.matmul_workspace_size(M, M, M, eng) + 1024, dtype=torch.uint8, device=dev)
                 ws = ws[(-ws.data_ptr()) % 1024:]
                 g.matmul_tc_prepare(A, B, M, M, M, ws, engine=eng)
-                for rows in rows_list:
+                for rows, hint in ((r, h) for r in rows_list for h in hints):
                     g.set_option("tc_group_rows", rows)
+                    g.set_option("tc_l2_hint", hint)
                     for _ in range(3):
                         g.matmul_tc_run(ws, M, M, M, C, engine=eng)
                     torch.cuda.synchronize()
@@ -1012,7 +1015,8 @@ def run_tc_sweep(args) -> None:
                     ms = e0.elapsed_time(e1) / n
                     mhz = clocks.get("sm_mhz")
                     work = PRODUCTS.get(eng, 1) * 2.0 * M ** 3
-                    print(json.dumps({"m": M, "engine": eng, "pair": pair, "group_rows": rows, "launches": n,
+                    print(json.dumps({"m": M, "engine": eng, "pair": pair, "group_rows": rows, "l2_hint": hint,
+                                      "launches": n,
                                       "ms": round(ms, 4), "tflops_fp32_work": round(2.0 * M ** 3 / ms / 1e9, 1),
                                       "tflops_tensor_work": round(work / ms / 1e9, 1), "sm_mhz": mhz,
                                       "mcycles": round(ms * mhz / 1e3, 3) if mhz else None,
@@ -1021,6 +1025,7 @@ def run_tc_sweep(args) -> None:
                 torch.cuda.empty_cache()
     g.set_option("tc_pair", 1)
     g.set_option("tc_group_rows", 2048)
+    g.set_option("tc_l2_hint", 0)
 
 
 def main():
@@ -1041,7 +1046,15 @@ def main():
     ap.add_argument("--sweep-group-rows", default="2048", help="raster group heights to sweep (multiples of 128)")
     ap.add_argument("--sweep-seconds", type=float, default=1.5)
     ap.add_argument("--sweep-pairs", default="1,0,2", help="tc_pair settings to sweep")
+    ap.add_argument("--sweep-l2-hints", default="0", help="tc_l2_hint settings to sweep")
+    ap.add_argument("--option", action="append", default=[], metavar="NAME=VALUE",
+                    help="gatlas_set_option before a --case or --tc-sweep run (repeatable)")
     args = ap.parse_args()
+    if args.option:
+        import gatlas_b200 as g
+        for o in args.option:
+            name, value = o.split("=", 1)
+            g.set_option(name, int(value))
     if args.tc_sweep:
         run_tc_sweep(args)
         return

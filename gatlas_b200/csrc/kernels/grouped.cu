@@ -27,6 +27,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <queue>
@@ -55,8 +56,26 @@ constexpr int kPackRows = 128;            // rows per pack item
 // 128-byte swizzle) and promotes after the same K as the single-instance
 // engine (all of K for one-product BF16, 256 for split3), issuing the same
 // MMA sequence, so that each instance's result is bit-identical to it.
-template <int MODE>
-using GLayout = tcg::Layout<MODE, kRowBytes>;
+// Ring layout: a stage holds every piece of a 128-row A tile and of BROWS
+// rows of B (128-byte K slices): all 256 rows of the widest tile on a single
+// CTA, its 128-row half on each CTA of a pair.
+template <int MODE, int BROWS>
+struct GLayout {
+    using MD = tcg::Mode<MODE>;
+    static constexpr int BK = kRowBytes / MD::ELEM;
+    static constexpr uint32_t SWIZZLE = tc::kSwizzle128B;
+    static constexpr uint32_t SBO = 8 * kRowBytes;
+    static constexpr int KSTEPS = kRowBytes / 32;
+    static constexpr uint32_t A_TILE = BM * kRowBytes;
+    static constexpr uint32_t B_TILE = BROWS * kRowBytes;
+    static constexpr uint32_t STAGE_BYTES = MD::NP * (A_TILE + B_TILE);
+    static constexpr int FIT = (int)((226 * 1024 - 1024) / STAGE_BYTES);
+    static constexpr int STAGES = FIT < 8 ? FIT : 8;
+    static constexpr uint32_t SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + alignment slack
+    static_assert(STAGES >= 2, "grouped pipeline depth");
+};
+template <int MODE, bool PAIR>
+using GLayoutOf = GLayout<MODE, PAIR ? 128 : 256>;
 constexpr int grouped_seg_kblocks(int mode) { return mode == 0 ? tcg::kSegAll : 256 / kBK; }
 
 // Packed byte offset of 16-byte chunk c of row `row` in K slice kb.
@@ -248,14 +267,23 @@ __global__ void __launch_bounds__(256, 2) grouped_pack_kernel(const Inst *insts,
 // ---------------------------------------------------------------------------
 struct Params {
     const TileRec *tiles;
-    const int32_t *cta_start;  // tiles of CTA b: [cta_start[b], cta_start[b+1])
+    const int32_t *cta_start;  // tiles of CTA (pair kernel: cluster) b: [cta_start[b], cta_start[b+1])
     int seg_kblocks;
     int *fault;
 };
 
-template <int MODE>
+// PAIR: a cluster of two CTAs runs 256 x bn tiles (an instance's row blocks
+// in pairs), the leader issuing cta_group::2 MMAs (M = 256) on both CTAs'
+// shared memory: each CTA stages its own 128-row A tile and half of the B
+// tile's rows, so at bn = 256 a CTA moves a third fewer operand bytes per MMA
+// than on a single-CTA 128 x 256 tile.
+// Each CTA's copies complete on its own barrier; the peer's warp 1 relays
+// every landed stage to the leader's barrier, which the MMA issuer waits on.
+// The leader's MMAs commit to both CTAs' ring and accumulator barriers; both
+// CTAs' drain warps (each on its own 128 rows of TMEM) arrive on the leader's.
+template <int MODE, bool PAIR>
 __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
-    using L = GLayout<MODE>;
+    using L = GLayoutOf<MODE, PAIR>;
     using MD = tcg::Mode<MODE>;
     constexpr int S = L::STAGES;
     static_assert(L::BK == kBK, "grouped engine stages BF16 slices of 64");
@@ -267,16 +295,24 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
     __shared__ int ring_issued, ring_consumed, mma_aborted;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int t_begin = p.cta_start[blockIdx.x], t_end = p.cta_start[blockIdx.x + 1];
+    const uint32_t rank = PAIR ? tc::cluster_ctarank() : 0u;
+    const bool leader = rank == 0;
+    const int unit = PAIR ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
+    const int t_begin = p.cta_start[unit], t_end = p.cta_start[unit + 1];
+    auto wait = [&](uint64_t *bar, uint32_t parity, uint64_t limit) {
+        return PAIR ? tc::wait_timed_cluster(bar, parity, limit, &abort_flag)
+                    : tc::wait_timed(bar, parity, limit, &abort_flag);
+    };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; ++s) {
-            mbar_init(&full[s], 1);
+            // the leader's stage completes on its own copies and the peer's relay
+            mbar_init(&full[s], PAIR && leader ? 2 : 1);
             mbar_init(&empty[s], 1);
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], kDrainWarps);
+            mbar_init(&tempty[b], (PAIR ? 2 : 1) * kDrainWarps);
         }
         mbar_init(&mma_done, 1);
         fence_mbarrier_init();
@@ -285,11 +321,17 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
         mma_aborted = 0;
     }
     if (warp == 0) {
-        tc::tmem_alloc(&tmem_base, kTmemCols);
-        tc::tmem_relinquish();
+        if constexpr (PAIR) {
+            tc::tmem_alloc_pair(&tmem_base, kTmemCols);
+            tc::tmem_relinquish_pair();
+        } else {
+            tc::tmem_alloc(&tmem_base, kTmemCols);
+            tc::tmem_relinquish();
+        }
     }
     tc::fence_before_sync();
     __syncthreads();
+    if constexpr (PAIR) tc::cluster_sync();  // both CTAs' barriers exist before any signal crosses the pair
     tc::fence_after_sync();
     const uint32_t tmem = tmem_base;
 
@@ -306,10 +348,16 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
             for (int t = t_begin; t < t_end && !stop; ++t) {
                 // the next record loads while this tile's copies are issued
                 const TileRec next = p.tiles[t + 1 < t_end ? t + 1 : t];
-                const uint32_t b_bytes = (uint32_t)cur.bn * kRowBytes;
+                // a slice of the B tile is bn rows, and a pair CTA copies its half of
+                // them; rank 1's A tile is the next row block, or (in a tile of 128
+                // rows or fewer) rank 0's again, whose products are never stored
+                const uint32_t b_slice = (uint32_t)cur.bn * kRowBytes;
+                const uint32_t b_bytes = PAIR ? b_slice / 2 : b_slice;
+                const int64_t a_off = (PAIR && rank == 1 && cur.rows > BM) ? (int64_t)cur.kt * kATileBytes : 0;
+                const int64_t b_off = PAIR ? (int64_t)rank * b_bytes : 0;
                 for (int kb = 0; kb < cur.kt; ++kb, ++ring) {
                     const int s = ring % S;
-                    if (!tc::wait_timed(&empty[s], ((uint32_t)(ring / S) & 1u) ^ 1u, kWaitNs, &abort_flag)) {
+                    if (!wait(&empty[s], ((uint32_t)(ring / S) & 1u) ^ 1u, kWaitNs)) {
                         if (!abort_flag) report_fault(p.fault, kFaultTcProducerWait);
                         abort_flag = 1;
                         stop = true;
@@ -317,8 +365,8 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
                     }
                     mbar_arrive_expect_tx(&full[s], MD::NP * (kATileBytes + b_bytes));
                     for (int i = 0; i < MD::NP; ++i) {
-                        bulk_g2s(a_tile(s, i), cur.a[i] + (int64_t)kb * kATileBytes, kATileBytes, &full[s]);
-                        bulk_g2s(b_tile(s, i), cur.b[i] + (int64_t)kb * b_bytes, b_bytes, &full[s]);
+                        bulk_g2s(a_tile(s, i), cur.a[i] + a_off + (int64_t)kb * kATileBytes, kATileBytes, &full[s]);
+                        bulk_g2s(b_tile(s, i), cur.b[i] + b_off + (int64_t)kb * b_slice, b_bytes, &full[s]);
                     }
                 }
                 cur = next;
@@ -327,8 +375,30 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
         }
         __syncwarp();
     } else if (warp == 1) {
-        if (lane == 0) {
+        if (PAIR && !leader && lane == 0) {
+            // ---- relay: each landed stage of this CTA, to the leader's barrier ----
+            const uint32_t full_leader = tc::mapa_shared(smem_u32(&full[0]), 0);
+            int ring = 0;
+            bool stop = false;
+            for (int t = t_begin; t < t_end && !stop; ++t) {
+                const int kt = p.tiles[t].kt;
+                for (int kb = 0; kb < kt; ++kb, ++ring) {
+                    const int s = ring % S;
+                    if (!wait(&full[s], (uint32_t)(ring / S) & 1u, kWaitNs)) {
+                        if (!abort_flag) report_fault(p.fault, kFaultTcProducerWait);
+                        abort_flag = 1;
+                        stop = true;
+                        break;
+                    }
+                    tc::mbar_arrive_remote(full_leader + (uint32_t)(s * sizeof(uint64_t)));
+                }
+            }
+        } else if (lane == 0) {
             // ---- MMA issuer ----
+            const uint32_t empty_self = PAIR ? tc::mapa_shared(smem_u32(&empty[0]), 0) : 0u;
+            const uint32_t empty_peer = PAIR ? tc::mapa_shared(smem_u32(&empty[0]), 1) : 0u;
+            const uint32_t tfull_self = PAIR ? tc::mapa_shared(smem_u32(&tfull[0]), 0) : 0u;
+            const uint32_t tfull_peer = PAIR ? tc::mapa_shared(smem_u32(&tfull[0]), 1) : 0u;
             int ring = 0, seg = 0;
             bool stop = false;
             int2 cur = make_int2(0, 0);  // (kt, bn)
@@ -337,14 +407,14 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
                 const int tn = t + 1 < t_end ? t + 1 : t;
                 const int2 next = make_int2(p.tiles[tn].kt, p.tiles[tn].bn);
                 const int kt = cur.x;
-                const uint32_t idesc = tc::idesc_bf16_f32(BM, cur.y);
+                const uint32_t idesc = tc::idesc_bf16_f32(PAIR ? 2 * BM : BM, cur.y);
                 cur = next;
                 for (int kb = 0; kb < kt; ++kb, ++ring) {
                     const int b = seg & 1;
                     const bool seg_first = (kb % p.seg_kblocks) == 0;
                     const bool seg_last = (kb % p.seg_kblocks) == p.seg_kblocks - 1 || kb == kt - 1;
                     if (seg_first) {
-                        if (!tc::wait_timed(&tempty[b], ((uint32_t)(seg >> 1) & 1u) ^ 1u, kWaitNs, &abort_flag)) {
+                        if (!wait(&tempty[b], ((uint32_t)(seg >> 1) & 1u) ^ 1u, kWaitNs)) {
                             if (!abort_flag) report_fault(p.fault, kFaultTcMmaWait);
                             abort_flag = 1;
                             stop = true;
@@ -353,7 +423,7 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
                         tc::fence_after_sync();
                     }
                     const int s = ring % S;
-                    if (!tc::wait_timed(&full[s], (uint32_t)(ring / S) & 1u, kWaitNs, &abort_flag)) {
+                    if (!wait(&full[s], (uint32_t)(ring / S) & 1u, kWaitNs)) {
                         if (!abort_flag) report_fault(p.fault, kFaultTcMmaWait);
                         abort_flag = 1;
                         stop = true;
@@ -367,23 +437,34 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
                         for (int j = 0; j < MD::NPROD; ++j) {
                             const uint32_t a_addr = smem_u32(a_tile(s, MD::pa(j))) + kk * 32;
                             const uint32_t b_addr = smem_u32(b_tile(s, MD::pb(j))) + kk * 32;
-                            tc::mma_bf16(d, tc::smem_desc_kmajor(a_addr, L::SBO, L::SWIZZLE),
-                                         tc::smem_desc_kmajor(b_addr, L::SBO, L::SWIZZLE), idesc,
-                                         (seg_first && kk == 0 && j == 0) ? 0u : 1u);
+                            const uint64_t ad = tc::smem_desc_kmajor(a_addr, L::SBO, L::SWIZZLE);
+                            const uint64_t bd = tc::smem_desc_kmajor(b_addr, L::SBO, L::SWIZZLE);
+                            const uint32_t accum = (seg_first && kk == 0 && j == 0) ? 0u : 1u;
+                            if constexpr (PAIR) tc::mma_bf16_pair(d, ad, bd, idesc, accum);
+                            else tc::mma_bf16(d, ad, bd, idesc, accum);
                         }
                     }
-                    tc::commit_to(&empty[s]);
-                    if (seg_last) {
-                        tc::commit_to(&tfull[b]);
-                        ++seg;
+                    if constexpr (PAIR) {
+                        const uint32_t so = (uint32_t)(s * sizeof(uint64_t)), bo = (uint32_t)(b * sizeof(uint64_t));
+                        tc::commit_pair_to(empty_self + so);
+                        tc::commit_pair_to(empty_peer + so);
+                        if (seg_last) {
+                            tc::commit_pair_to(tfull_self + bo);
+                            tc::commit_pair_to(tfull_peer + bo);
+                        }
+                    } else {
+                        tc::commit_to(&empty[s]);
+                        if (seg_last) tc::commit_to(&tfull[b]);
                     }
+                    if (seg_last) ++seg;
                 }
             }
             ring_consumed = ring;
             if (stop) {
                 // every MMA issued before the abort completes before TMEM is freed
                 mma_aborted = 1;
-                tc::commit_to(&mma_done);
+                if constexpr (PAIR) tc::commit_pair_to(tc::mapa_shared(smem_u32(&mma_done), 0));
+                else tc::commit_to(&mma_done);
             }
         }
         __syncwarp();
@@ -391,6 +472,8 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
         // ---- drain + epilogue ----
         const int quarter = warp & 3, half = (warp - 2) >> 2;
         const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+        const int row_off = PAIR ? (int)rank * 128 : 0;  // a pair CTA's rows of the 256-row tile
+        const uint32_t tempty_leader = PAIR ? tc::mapa_shared(smem_u32(&tempty[0]), 0) : 0u;
         int seg = 0;
         bool ok = true;
         for (int t = t_begin; t < t_end && ok; ++t) {
@@ -412,7 +495,7 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
             {
                 // C is read by the epilogue (beta != 0): pull this warp's rows
                 // of it into L2 while the tile's MMAs run
-                const int r = quarter * 32 + lane;
+                const int r = row_off + quarter * 32 + lane;
                 if (R->gemm && R->beta != 0.0f && r < R->rows) {
                     const int left = R->cols - half * hw;
                     const int ncols = left < hw ? left : hw;
@@ -423,7 +506,7 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
             }
             for (int sg = 0; sg < nseg; ++sg, ++seg) {
                 const int b = seg & 1;
-                if (!tc::wait_timed(&tfull[b], (uint32_t)(seg >> 1) & 1u, 2 * kWaitNs, &abort_flag)) {
+                if (!wait(&tfull[b], (uint32_t)(seg >> 1) & 1u, 2 * kWaitNs)) {
                     if (!abort_flag) report_fault(p.fault, kFaultTcEpilogueWait);
                     abort_flag = 1;
                     ok = false;
@@ -449,7 +532,10 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
                 }
                 tc::fence_before_sync();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&tempty[b]);
+                if (lane == 0) {
+                    if (!PAIR || leader) mbar_arrive(&tempty[b]);
+                    else tc::mbar_arrive_remote(tempty_leader + (uint32_t)(b * sizeof(uint64_t)));
+                }
             }
             if (!ok || abort_flag) break;
             const int left = R->cols - half * hw;
@@ -463,7 +549,7 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
             for (int rs = 0; rs < 2; ++rs) {
 #pragma unroll
                 for (int rr = 0; rr < 2; ++rr) {
-                    const int row = quarter * 32 + rs * 16 + (lane >> 2) + 8 * rr;
+                    const int row = row_off + quarter * 32 + rs * 16 + (lane >> 2) + 8 * rr;
                     if (row >= R->rows) continue;
                     float *cp = R->C + (int64_t)row * R->ldc + half * hw;
                     // four 8-column groups at a time: their loads of C
@@ -509,13 +595,27 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
     tc::fence_before_sync();
     __syncthreads();
     if (threadIdx.x == 0 && abort_flag) {
-        // bounded waits for the copies still landing and the MMAs issued before the abort
-        for (int r = ring_consumed; r < ring_issued; ++r)
-            tc::wait_timed(&full[r % S], (uint32_t)(r / S) & 1u, kWaitNs, nullptr);
-        if (mma_aborted) tc::wait_timed(&mma_done, 0, kWaitNs, nullptr);
+        if constexpr (PAIR) {
+            // a pair's stages complete on two CTAs' barriers: give every copy in
+            // flight time to land (microseconds), then the MMAs issued before the abort
+            const uint64_t t0 = tc::globaltimer();
+            while (tc::globaltimer() - t0 < 20000000ull) {
+            }
+            if (leader && mma_aborted) tc::wait_timed(&mma_done, 0, kWaitNs, nullptr);
+        } else {
+            // bounded waits for the copies still landing and the MMAs issued before the abort
+            for (int r = ring_consumed; r < ring_issued; ++r)
+                tc::wait_timed(&full[r % S], (uint32_t)(r / S) & 1u, kWaitNs, nullptr);
+            if (mma_aborted) tc::wait_timed(&mma_done, 0, kWaitNs, nullptr);
+        }
     }
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, kTmemCols);
+    if constexpr (PAIR) {
+        tc::cluster_sync();  // neither CTA leaves while the pair can still touch its memory
+        if (warp == 0) tc::tmem_dealloc_pair(tmem, kTmemCols);
+    } else {
+        if (warp == 0) tc::tmem_dealloc(tmem, kTmemCols);
+    }
 }
 
 }  // namespace grp
@@ -531,6 +631,8 @@ int32_t g_tile_table[2][kGroupedBuckets] = {{64, 128, 256, 256}, {64, 128, 256, 
 
 int engine_slot(int engine) { return engine == GATLAS_ENGINE_TC_SPLIT3 ? 1 : 0; }
 
+std::atomic<int> g_pair_mode{0};
+
 size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 }  // namespace
@@ -542,6 +644,45 @@ int32_t grouped_bucket(int64_t m, int64_t n, int64_t k) {
     if (n <= 128) return 1;
     if (n <= 256) return 2;
     return 3;
+}
+
+int grouped_set_pair(int mode) {
+    if (mode < 0 || mode > 1) return set_error(GATLAS_ERR_INVALID, "grouped_pair: %d (0 single CTAs, 1 CTA pairs)", mode);
+    g_pair_mode.store(mode);
+    return GATLAS_OK;
+}
+
+int grouped_get_pair() { return g_pair_mode.load(); }
+
+// Clusters of two that fit at once (occupancy query, once per device).
+template <int MODE>
+static int pair_units_cap() {
+    static thread_local int cap_dev = -1, cap = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cap_dev != dev) {
+        auto kern = grp::grouped_gemm_kernel<MODE, true>;
+        cap = sm_count() / 2;
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)grp::GLayoutOf<MODE, true>::SMEM_BYTES) == cudaSuccess) {
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = 2;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3(2 * (unsigned)cap, 1, 1);
+            cfg.blockDim = dim3(grp::kThreads, 1, 1);
+            cfg.dynamicSmemBytes = grp::GLayoutOf<MODE, true>::SMEM_BYTES;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            int n = 0;
+            if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) == cudaSuccess && n > 0) cap = n;
+        }
+        cudaGetLastError();
+        cap_dev = dev;
+    }
+    return std::max(cap, 1);
 }
 
 int grouped_set_tile_table(int engine, const int32_t *t, int32_t nb) {
@@ -623,11 +764,15 @@ int grouped_build(int engine, const gatlas_grouped_instance *in, int32_t count, 
         grp::TileRec r;
     };
     std::vector<Cand> cands;
+    for (int i = 0; i < count; ++i) {
+        int rc = resolve_instance(in[i], engine_slot(engine), &t->ip[i]);
+        if (rc) return rc;
+    }
+    t->pair = g_pair_mode.load() == 1;
+    const int step_m = t->pair ? 2 : 1;
     size_t off = 0;
     for (int i = 0; i < count; ++i) {
         InstPlan &o = t->ip[i];
-        int rc = resolve_instance(in[i], engine_slot(engine), &o);
-        if (rc) return rc;
         const gatlas_grouped_instance &q = in[i];
         if (q.m > 0 && q.n > 0 && (!q.c || (q.k > 0 && (!q.a || !q.b))))
             return set_error(GATLAS_ERR_INVALID, "grouped: instance %d has a null pointer", i);
@@ -655,13 +800,14 @@ int grouped_build(int engine, const gatlas_grouped_instance *in, int32_t count, 
         t->seg[2 * i + 2] = t->seg[2 * i + 1] + b_items;
         // cost in bytes moved: operand tiles through shared memory plus the C
         // tile (read too when beta != 0), plus a fixed per-tile overhead
-        const int64_t c_bytes = (int64_t)grp::BM * o.bn * 4 * ((q.gemm && q.beta != 0.0) ? 2 : 1);
-        const int64_t cost = (int64_t)o.kt * t->np * (grp::BM + o.bn) * grp::kRowBytes + c_bytes + 16384;
+        // (a pair tile: both CTAs' halves, as one unit of its cluster's time)
+        const int64_t c_bytes = (int64_t)step_m * grp::BM * o.bn * 4 * ((q.gemm && q.beta != 0.0) ? 2 : 1);
+        const int64_t cost = (int64_t)o.kt * t->np * (step_m * grp::BM + o.bn) * grp::kRowBytes + c_bytes + 16384;
         // grouped raster inside the instance: 16 tile rows per group, so the
         // tiles that run at the same time share A and B rows through L2
         for (int g0 = 0; g0 < o.mt; g0 += 16)
             for (int tn = 0; tn < o.nt; ++tn)
-                for (int tm = g0; tm < std::min(o.mt, g0 + 16); ++tm) {
+                for (int tm = g0; tm < std::min(o.mt, g0 + 16); tm += step_m) {
                 grp::TileRec r;
                 std::memset(&r, 0, sizeof(r));
                 for (int j = 0; j < t->np && pb; ++j) {
@@ -672,7 +818,7 @@ int grouped_build(int engine, const gatlas_grouped_instance *in, int32_t count, 
                 r.ldc = o.ldc;
                 r.kt = o.kt;
                 r.bn = o.bn;
-                r.rows = (int32_t)std::min<int64_t>(grp::BM, o.M - (int64_t)tm * grp::BM);
+                r.rows = (int32_t)std::min<int64_t>(step_m * grp::BM, o.M - (int64_t)tm * grp::BM);
                 r.cols = (int32_t)std::min<int64_t>(o.bn, o.N - (int64_t)tn * o.bn);
                 r.alpha = (float)q.alpha;
                 r.beta = (float)q.beta;
@@ -685,7 +831,8 @@ int grouped_build(int engine, const gatlas_grouped_instance *in, int32_t count, 
     t->ntiles = (int64_t)cands.size();
     // longest first onto the least-loaded CTA
     std::stable_sort(cands.begin(), cands.end(), [](const Cand &a, const Cand &b) { return a.cost > b.cost; });
-    t->grid = (int)std::min<int64_t>(sm_count(), std::max<int64_t>(t->ntiles, 1));
+    const int units = t->pair ? (t->mode == 1 ? pair_units_cap<1>() : pair_units_cap<0>()) : sm_count();
+    t->grid = (int)std::min<int64_t>(units, std::max<int64_t>(t->ntiles, 1));
     std::vector<int> owner(cands.size());
     std::vector<int32_t> count_per(t->grid, 0);
     {
@@ -737,30 +884,58 @@ int grouped_launch_pack(const GroupedTables &t, const GroupedDevice &d, cudaStre
     return check_launch("grouped_pack_kernel");
 }
 
-template <int MODE>
+// Shared-memory attributes of the four contraction kernels, once per device
+// (also before a graph capture, since attribute changes are not captured).
+static int grouped_gemm_attributes() {
+    static thread_local int attr_dev = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (attr_dev == dev) return GATLAS_OK;
+    const cudaError_t e[4] = {
+        cudaFuncSetAttribute(grp::grouped_gemm_kernel<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)grp::GLayoutOf<0, false>::SMEM_BYTES),
+        cudaFuncSetAttribute(grp::grouped_gemm_kernel<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)grp::GLayoutOf<1, false>::SMEM_BYTES),
+        cudaFuncSetAttribute(grp::grouped_gemm_kernel<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)grp::GLayoutOf<0, true>::SMEM_BYTES),
+        cudaFuncSetAttribute(grp::grouped_gemm_kernel<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)grp::GLayoutOf<1, true>::SMEM_BYTES)};
+    for (cudaError_t x : e)
+        if (x != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "grouped smem attribute: %s", cudaGetErrorString(x));
+    attr_dev = dev;
+    return GATLAS_OK;
+}
+
+template <int MODE, bool PAIR>
 static int launch_grouped(const GroupedTables &t, const GroupedDevice &d, cudaStream_t stream) {
-    using L = grp::GLayout<MODE>;
     grp::Params prm;
     prm.tiles = d.tiles;
     prm.cta_start = d.cta;
     prm.seg_kblocks = grp::grouped_seg_kblocks(MODE);
     prm.fault = device_fault_word();
-    const int smem = (int)L::SMEM_BYTES;
-    static thread_local int attr_set[2] = {-1, -1};  // device whose attribute was set
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (attr_set[MODE] != dev) {
-        cudaError_t e = cudaFuncSetAttribute(grp::grouped_gemm_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "grouped smem attribute: %s", cudaGetErrorString(e));
-        attr_set[MODE] = dev;
-    }
-    grp::grouped_gemm_kernel<MODE><<<t.grid, grp::kThreads, smem, stream>>>(prm);
+    const int rc = grouped_gemm_attributes();
+    if (rc) return rc;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)((PAIR ? 2 : 1) * t.grid), 1, 1);
+    cfg.blockDim = dim3(grp::kThreads, 1, 1);
+    cfg.dynamicSmemBytes = grp::GLayoutOf<MODE, PAIR>::SMEM_BYTES;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = PAIR ? 1 : 0;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, grp::grouped_gemm_kernel<MODE, PAIR>, prm);
+    if (e != cudaSuccess) return set_error(GATLAS_ERR_CUDA, "grouped_gemm_kernel: %s", cudaGetErrorString(e));
     return check_launch("grouped_gemm_kernel");
 }
 
 int grouped_launch_contract(const GroupedTables &t, const GroupedDevice &d, cudaStream_t stream) {
     if (t.ntiles == 0) return GATLAS_OK;
-    return t.mode == 1 ? launch_grouped<1>(t, d, stream) : launch_grouped<0>(t, d, stream);
+    if (t.pair) return t.mode == 1 ? launch_grouped<1, true>(t, d, stream) : launch_grouped<0, true>(t, d, stream);
+    return t.mode == 1 ? launch_grouped<1, false>(t, d, stream) : launch_grouped<0, false>(t, d, stream);
 }
 
 struct GroupedPlan {
@@ -901,10 +1076,11 @@ int grouped_launch_graph(GroupedPlan *p, int with_prepare, cudaStream_t stream) 
         if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess)
             return set_error(GATLAS_ERR_CUDA, "grouped: capture stream");
         // attribute changes are not captured: set them before the capture
-        cudaFuncSetAttribute(grp::grouped_gemm_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)grp::GLayout<0>::SMEM_BYTES);
-        cudaFuncSetAttribute(grp::grouped_gemm_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)grp::GLayout<1>::SMEM_BYTES);
+        const int arc = grouped_gemm_attributes();
+        if (arc) {
+            cudaStreamDestroy(cap);
+            return arc;
+        }
         grouped_pack_attributes();
         device_fault_word();
         cudaGraph_t graph = nullptr;
@@ -972,7 +1148,7 @@ int grouped_run_each(GroupedPlan *p, cudaStream_t stream) {
 int grouped_info(const GroupedPlan *p, int64_t *tiles, int32_t *ctas, double *flops, int64_t *items) {
     if (!p) return set_error(GATLAS_ERR_INVALID, "grouped: null plan");
     if (tiles) *tiles = p->t.ntiles;
-    if (ctas) *ctas = p->t.grid;
+    if (ctas) *ctas = p->t.grid * (p->t.pair ? 2 : 1);
     if (flops) *flops = p->t.flops;
     if (items) *items = p->t.nitems;
     return GATLAS_OK;

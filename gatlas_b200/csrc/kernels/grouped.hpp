@@ -51,6 +51,7 @@ struct InstPlan {
 // output tile records in CTA order and each CTA's range (contraction).
 struct GroupedTables {
     int engine = 0, np = 1, mode = 0;
+    bool pair = false;  // 256-row tiles on CTA pairs; `grid` and `cta` count clusters
     std::vector<InstPlan> ip;
     std::vector<grp::Inst> inst;
     std::vector<int64_t> seg;
@@ -87,6 +88,10 @@ GroupedDevice grouped_tables_device(const GroupedTables &t, const void *dev_base
 struct GroupedPlan;
 
 int32_t grouped_bucket(int64_t m, int64_t n, int64_t k);
+// Tiling of grouped contractions: 0 128-row tiles on single CTAs (the
+// default), 1 256-row tiles on CTA pairs.
+int grouped_set_pair(int mode);
+int grouped_get_pair();
 int grouped_set_tile_table(int engine, const int32_t *t, int32_t nb);
 int grouped_get_tile_table(int engine, int32_t *t, int32_t nb);
 size_t grouped_workspace_bytes(int engine, const gatlas_grouped_instance *in, int32_t count);

@@ -266,6 +266,38 @@ __device__ __forceinline__ void tma_load_3d_pair(void *smem_dst, const void *tma
         : "memory");
 }
 
+// L2 eviction priorities for cache-hinted loads (createpolicy, whole range).
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+__device__ __forceinline__ uint64_t l2_policy_evict_first() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+// tma_load_3d / tma_load_3d_pair with an L2 eviction priority.
+__device__ __forceinline__ void tma_load_3d_hint(void *smem_dst, const void *tmap, int32_t x, int32_t y, int32_t z,
+                                                 uint64_t *bar, uint64_t policy) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cta.global.tile.mbarrier::complete_tx::bytes.L2::cache_hint"
+        " [%0], [%1, {%2, %3, %4}], [%5], %6;" ::"r"(smem_u32(smem_dst)),
+        "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar)), "l"(policy)
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d_pair_hint(void *smem_dst, const void *tmap, int32_t x, int32_t y,
+                                                      int32_t z, uint32_t bar_cluster_addr, uint64_t policy) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+        " [%0], [%1, {%2, %3, %4}], [%5], %6;" ::"r"(smem_u32(smem_dst)),
+        "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(bar_cluster_addr), "l"(policy)
+        : "memory");
+}
+
 #endif  // __CUDACC__
 
 }  // namespace tc

@@ -201,6 +201,26 @@ def test_raster_group_height_does_not_change_results(cuda, engine, rows):
         assert oracle.normwise_error(got, ref) <= BUDGET[engine]
 
 
+@pytest.mark.parametrize("engine", ENGINES + ["tc_fp8"])
+@pytest.mark.parametrize("hint", [1, 2])
+@pytest.mark.parametrize("pair", [0, 2])
+def test_l2_hints_do_not_change_results(cuda, engine, hint, pair):
+    # eviction priorities on the operand loads change what stays in L2, not
+    # what is loaded: single CTAs and CTA pairs, batched, ragged edges
+    M, N, K, P = 700, 520, 400, 2
+    A = oracle.uniform(P * M * K, seed=41)
+    B = oracle.uniform(P * K * N, seed=42)
+    try:
+        g.set_option("tc_pair", pair)
+        base = _mm(cuda, A, B, M, N, K, engine, batch=P)
+        g.set_option("tc_l2_hint", hint)
+        got = _mm(cuda, A, B, M, N, K, engine, batch=P)
+    finally:
+        g.set_option("tc_l2_hint", 0)
+        g.set_option("tc_pair", 1)
+    assert np.array_equal(base, got)
+
+
 @pytest.mark.parametrize("engine", ENGINES + ["tc_fp8", "buffer"])
 @pytest.mark.parametrize("ta,tb", [(0, 0), (1, 1), (1, 0)])
 def test_host_buffer_entry_matches_device_path(cuda, engine, ta, tb):

@@ -69,6 +69,38 @@ def test_grouped_equals_single_instance_engine(cuda, engine):
     plan.close()
 
 
+@pytest.fixture
+def pair_option():
+    old = g.get_option("grouped_pair")
+    yield
+    g.set_option("grouped_pair", old)
+
+
+@pytest.mark.parametrize("engine", ["tc_bf16", "tc_split3"])
+def test_cta_pairs_equal_single_ctas(cuda, engine, pair_option):
+    # 256-row tiles on CTA pairs against 128-row tiles on single CTAs: odd and
+    # even counts of row blocks, every tile width, ragged edges
+    rng = np.random.default_rng(21)
+    shapes = SHAPES + [(int(rng.integers(1, 900)), int(rng.integers(1, 700)), int(rng.integers(1, 400)),
+                        int(rng.integers(0, 2)), int(rng.integers(0, 2)), int(rng.integers(0, 2)), 1.25,
+                        float(rng.integers(0, 2)), int(rng.choice([0, 64, 128, 256]))) for _ in range(24)]
+    inst = _make(cuda, shapes, seed=21)
+    g.set_option("grouped_pair", 0)
+    single = g.Grouped(inst, engine=engine)
+    single.prepare().run()
+    want = _results(inst)
+    g.set_option("grouped_pair", 1)
+    pair = g.Grouped(inst, engine=engine)
+    assert pair.info()["ctas"] % 2 == 0 and pair.info()["tiles"] < single.info()["tiles"]
+    for launch in (lambda: pair.prepare().run(), lambda: pair.launch_graph(with_prepare=True)):
+        _reset(inst)
+        launch()
+        for q, x, y in zip(inst, _results(inst), want):
+            assert np.array_equal(x, y), (q["m"], q["n"], q["k"], q["tile_n"])
+    single.close()
+    pair.close()
+
+
 @pytest.mark.parametrize("tile_n", [64, 128, 256])
 def test_result_independent_of_tile_width(cuda, tile_n):
     shapes = [(200, 300, 100, 0, 1, 1, 0.5, 1.0, tile_n), (77, 45, 260, 1, 0, 0, 1.0, 0.0, tile_n)]

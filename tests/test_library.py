@@ -82,6 +82,17 @@ def test_options_round_trip_without_a_device():
         g.set_option("no_such_option", 1)
     with pytest.raises(g.GatlasError, match="0, 1 or 2"):
         g.set_option("tc_pair", 3)
+    assert g.get_option("tc_l2_hint") == 0
+    with pytest.raises(g.GatlasError, match="0, 1 or 2"):
+        g.set_option("tc_l2_hint", 3)
+    assert g.get_option("grouped_pair") == 0
+    g.set_option("grouped_pair", 1)
+    try:
+        assert g.get_option("grouped_pair") == 1
+    finally:
+        g.set_option("grouped_pair", 0)
+    with pytest.raises(g.GatlasError, match="single CTAs"):
+        g.set_option("grouped_pair", 2)
     assert g.get_option("tc_group_rows") == 2048
     g.set_option("tc_group_rows", 384)
     try:
