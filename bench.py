@@ -969,8 +969,8 @@ def run_tc_sweep(args) -> None:
     sampled through NVML.  One JSON line per point; cycles = ms x median MHz.
     Pair settings (gatlas_set_option "tc_pair"): 1 the default choice (CTA
     pairs for split3/split6, 256 x 256 single-CTA tiles for BF16), 0 single
-    CTAs on 128 x 256 tiles, 2 CTA pairs.  L2 hints ("tc_l2_hint"): 0 none,
-    1 A evict-last and B evict-first, 2 the opposite."""
+    CTAs on 128 x 256 tiles, 2 CTA pairs.  L2 hint ("tc_l2_hint"): 1 (the
+    default) A's loads evict-last, 0 none."""
     import time
 
     import torch
@@ -1025,7 +1025,7 @@ def run_tc_sweep(args) -> None:
                 torch.cuda.empty_cache()
     g.set_option("tc_pair", 1)
     g.set_option("tc_group_rows", 2048)
-    g.set_option("tc_l2_hint", 0)
+    g.set_option("tc_l2_hint", 1)
 
 
 def main():
@@ -1046,7 +1046,7 @@ def main():
     ap.add_argument("--sweep-group-rows", default="2048", help="raster group heights to sweep (multiples of 128)")
     ap.add_argument("--sweep-seconds", type=float, default=1.5)
     ap.add_argument("--sweep-pairs", default="1,0,2", help="tc_pair settings to sweep")
-    ap.add_argument("--sweep-l2-hints", default="0", help="tc_l2_hint settings to sweep")
+    ap.add_argument("--sweep-l2-hints", default="1", help="tc_l2_hint settings to sweep")
     ap.add_argument("--option", action="append", default=[], metavar="NAME=VALUE",
                     help="gatlas_set_option before a --case or --tc-sweep run (repeatable)")
     args = ap.parse_args()

@@ -541,7 +541,8 @@ def set_option(name: str, value: int) -> None:
     """Library options (see gatlas_set_option in include/gatlas.h): "tc_pair"
     (tiling of tensor-core contractions: 1 default, 0 128 x 256 tiles, 2 CTA
     pairs), "tc_group_rows" (raster group height, multiple of 128),
-    "host_block_rows" (row block of the host-buffer pipeline, multiple of 256)
+    "host_block_rows" (row block of the host-buffer pipeline, multiple of 256),
+    "tc_l2_hint" (1 default: A's tiles evict-last in L2; 0 plain loads)
     and "grouped_pair" (grouped contractions on CTA pairs: 1, or single CTAs:
     0, the default)."""
     check(lib().gatlas_set_option(name.encode(), int(value)))

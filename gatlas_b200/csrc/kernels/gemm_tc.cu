@@ -70,9 +70,8 @@ struct Params {
     int tiles_m, tiles_n, batch;
     int tma_store;
     int group_tiles;  // tile rows per raster group
-    // L2 eviction priority of the operand loads: 0 none; 1 A (reused by every
-    // tile column of a raster group) evict-last, B (read by the group's tile
-    // rows at about the same time) evict-first; 2 the opposite
+    // 1: A's loads evict-last in L2 (A is reused by every tile column of a
+    // raster group, B by the group's tile rows at about the same time)
     int l2_hint;
     // FP8 persistent kernel: per tile (instance-major, then tile row, then
     // tile column) the segment count, one segment-start bit per 128-deep
@@ -205,9 +204,7 @@ __global__ void __launch_bounds__(kThreads2, 1)
         if (lane == 0) {
             // ---- TMA producer: one ring position per K slice, across tiles ----
             const uint32_t full_leader = PAIR ? tc::mapa_shared(smem_u32(&full[0]), 0) : 0u;
-            const uint64_t pol_last = tc::l2_policy_evict_last(), pol_first = tc::l2_policy_evict_first();
-            const uint64_t pol_a = p.l2_hint == 1 ? pol_last : pol_first;
-            const uint64_t pol_b = p.l2_hint == 1 ? pol_first : pol_last;
+            const uint64_t pol_a = tc::l2_policy_evict_last();
             int s = 0;
             uint32_t ph = 0;
             bool stop = false;
@@ -227,24 +224,16 @@ __global__ void __launch_bounds__(kThreads2, 1)
                         if (leader) mbar_arrive_expect_tx(&full[s], 2 * L::STAGE_BYTES);
                         const uint32_t bar = full_leader + (uint32_t)(s * sizeof(uint64_t));
                         for (int i = 0; i < MD::NP; ++i) {
-                            if (p.l2_hint) {
-                                tc::tma_load_3d_pair_hint(a_tile(s, i), tA[i], kb * BK, m0, z, bar, pol_a);
-                                tc::tma_load_3d_pair_hint(b_tile(s, i), tB[i], kb * BK, nb, z, bar, pol_b);
-                            } else {
-                                tc::tma_load_3d_pair(a_tile(s, i), tA[i], kb * BK, m0, z, bar);
-                                tc::tma_load_3d_pair(b_tile(s, i), tB[i], kb * BK, nb, z, bar);
-                            }
+                            if (p.l2_hint) tc::tma_load_3d_pair_hint(a_tile(s, i), tA[i], kb * BK, m0, z, bar, pol_a);
+                            else tc::tma_load_3d_pair(a_tile(s, i), tA[i], kb * BK, m0, z, bar);
+                            tc::tma_load_3d_pair(b_tile(s, i), tB[i], kb * BK, nb, z, bar);
                         }
                     } else {
                         mbar_arrive_expect_tx(&full[s], L::STAGE_BYTES);
                         for (int i = 0; i < MD::NP; ++i) {
-                            if (p.l2_hint) {
-                                tc::tma_load_3d_hint(a_tile(s, i), tA[i], kb * BK, m0, z, &full[s], pol_a);
-                                tc::tma_load_3d_hint(b_tile(s, i), tB[i], kb * BK, nb, z, &full[s], pol_b);
-                            } else {
-                                tma_load_3d(a_tile(s, i), tA[i], kb * BK, m0, z, &full[s]);
-                                tma_load_3d(b_tile(s, i), tB[i], kb * BK, nb, z, &full[s]);
-                            }
+                            if (p.l2_hint) tc::tma_load_3d_hint(a_tile(s, i), tA[i], kb * BK, m0, z, &full[s], pol_a);
+                            else tma_load_3d(a_tile(s, i), tA[i], kb * BK, m0, z, &full[s]);
+                            tma_load_3d(b_tile(s, i), tB[i], kb * BK, nb, z, &full[s]);
                         }
                     }
                     if (++s == S) {
@@ -1117,8 +1106,10 @@ static WsPtrs ws_ptrs(const Plan &pl, void *ws) {
 static int g_tc_pair = 1;
 // Rows of C per raster group of the persistent kernels (multiple of 128).
 static int g_tc_group_rows = kGroupM * 128;
-// L2 eviction priority of the persistent kernel's operand loads (Params::l2_hint).
-static int g_tc_l2_hint = 0;
+// A's loads evict-last in the persistent kernel (Params::l2_hint): at 8192^3
+// split3 on CTA pairs, 2.54 GB of DRAM reads per launch instead of 3.45, at the
+// same speed.
+static int g_tc_l2_hint = 1;
 
 // FP8 segment plan, one thread per tile: a run of at most seg_kblocks
 // 128-deep blocks whose scale products sa * sb are equal for every 128 x 128
@@ -1640,7 +1631,7 @@ extern "C" int gatlas_set_option(const char *name, int64_t value) {
         return GATLAS_OK;
     }
     if (std::strcmp(name, "tc_l2_hint") == 0) {
-        if (value < 0 || value > 2) return set_error(GATLAS_ERR_INVALID, "set_option: tc_l2_hint is 0, 1 or 2");
+        if (value < 0 || value > 1) return set_error(GATLAS_ERR_INVALID, "set_option: tc_l2_hint is 0 or 1");
         tcg::g_tc_l2_hint = (int)value;
         return GATLAS_OK;
     }

@@ -44,26 +44,32 @@ namespace gatlas {
 namespace grp {
 
 using tcg::BM;
-constexpr int kBK = 64;                  // BF16 elements per K slice
-constexpr uint32_t kRowBytes = 128;       // one K slice of one row
+constexpr int kPackBK = 64;              // K elements per pack item
+constexpr uint32_t kPackRowBytes = 128;   // one pack item's row of one BF16 piece
+constexpr uint32_t kRowBytes = 128;       // one contraction K slice of one row (128-byte swizzle)
+constexpr int kBK = kRowBytes / 2;        // BF16 elements per contraction K slice
+constexpr int kSlicesPerItem = (int)(kPackRowBytes / kRowBytes);
 constexpr uint32_t kATileBytes = BM * kRowBytes;
 constexpr int kDrainWarps = 8;
 constexpr int kThreads = 32 * (2 + kDrainWarps);
 constexpr uint32_t kTmemCols = 512;       // two accumulators of up to 256 columns
 constexpr uint64_t kWaitNs = 2000000000ull;
 constexpr int kPackRows = 128;            // rows per pack item
-// The grouped engine stages 128-byte K slices (its packed tiles carry the
-// 128-byte swizzle) and promotes after the same K as the single-instance
+constexpr int kEpiBatch = 8;              // 8-column groups of C loaded together by the epilogue
+// The grouped engine stages 64-byte K slices (its packed tiles carry the
+// 64-byte swizzle), so that a ring of 48 KiB stages holds four split3 K slices
+// of a 128 x 256 tile, and promotes after the same K as the single-instance
 // engine (all of K for one-product BF16, 256 for split3), issuing the same
-// MMA sequence, so that each instance's result is bit-identical to it.
+// MMA sequence (16-deep K steps in order, the products of each in order), so
+// that each instance's result is bit-identical to it.
 // Ring layout: a stage holds every piece of a 128-row A tile and of BROWS
-// rows of B (128-byte K slices): all 256 rows of the widest tile on a single
-// CTA, its 128-row half on each CTA of a pair.
+// rows of B (one K slice): all 256 rows of the widest tile on a single CTA,
+// its 128-row half on each CTA of a pair.
 template <int MODE, int BROWS>
 struct GLayout {
     using MD = tcg::Mode<MODE>;
     static constexpr int BK = kRowBytes / MD::ELEM;
-    static constexpr uint32_t SWIZZLE = tc::kSwizzle128B;
+    static constexpr uint32_t SWIZZLE = kRowBytes == 128 ? tc::kSwizzle128B : tc::kSwizzle64B;
     static constexpr uint32_t SBO = 8 * kRowBytes;
     static constexpr int KSTEPS = kRowBytes / 32;
     static constexpr uint32_t A_TILE = BM * kRowBytes;
@@ -78,10 +84,18 @@ template <int MODE, bool PAIR>
 using GLayoutOf = GLayout<MODE, PAIR ? 128 : 256>;
 constexpr int grouped_seg_kblocks(int mode) { return mode == 0 ? tcg::kSegAll : 256 / kBK; }
 
-// Packed byte offset of 16-byte chunk c of row `row` in K slice kb.
+// Packed byte offset of 16-byte chunk c (0..7) of row `row` of pack item kb
+// (K elements 64 kb .. 64 kb + 63) in an operand of kt items per row block of
+// tr rows.  Each row block is a run of K slices, each slice tr rows of
+// kRowBytes; 16-byte chunk j of row r sits at chunk j ^ (r & 7) (128-byte
+// swizzle) or j ^ ((r >> 1) & 3) (64-byte swizzle), the layouts the MMA's
+// shared-memory descriptors read.
 __device__ __forceinline__ int64_t packed_offset(int64_t row, int kb, int c, int tr, int kt) {
-    return ((row / tr) * kt + kb) * (int64_t)tr * kRowBytes + (row % tr) * kRowBytes +
-           ((c ^ (int)(row & 7)) << 4);
+    constexpr int per = (int)(kRowBytes / 16);  // chunks per slice row
+    const int s = kb * kSlicesPerItem + c / per, j = c % per;
+    const int swz = kRowBytes == 128 ? (int)(row & 7) : (int)((row >> 1) & 3);
+    return ((row / tr) * (int64_t)(kt * kSlicesPerItem) + s) * (int64_t)tr * kRowBytes + (row % tr) * kRowBytes +
+           ((j ^ swz) << 4);
 }
 
 // ---------------------------------------------------------------------------
@@ -108,7 +122,7 @@ __device__ __forceinline__ PackItem pack_item(const Inst *insts, const int64_t *
     const int64_t local = it - seg_start[sgi];
     q.kb = (int)(local % I.kt);
     q.r0 = (local / I.kt) * kPackRows;
-    q.k0 = (int64_t)q.kb * kBK;
+    q.k0 = (int64_t)q.kb * kPackBK;
     q.rows = q.op ? I.N : I.M;
     q.tr = q.op ? I.bn : BM;
     q.rows_alloc = q.op ? (int64_t)I.nt * I.bn : (int64_t)I.mt * BM;
@@ -124,7 +138,7 @@ __device__ __forceinline__ PackItem pack_item(const Inst *insts, const int64_t *
 // sources, [64 k][128 rows] (k rows of 512 B) for transposed ones, where the
 // 16-byte chunk of rows 4q..4q+3 in k row k sits at chunk q ^ ((k >> 3) & 7),
 // so that the eight k-runs one warp reads per row land in distinct banks.
-constexpr uint32_t kPackTileBytes = kPackRows * kBK * 4;
+constexpr uint32_t kPackTileBytes = kPackRows * kPackBK * 4;
 constexpr int kPackStages = 3;
 constexpr uint32_t kPackSmemBytes = kPackStages * kPackTileBytes;
 constexpr int kPackChunks = (int)(kPackTileBytes / 16) / 256;  // 16-byte chunks per thread per item
@@ -221,7 +235,7 @@ __global__ void __launch_bounds__(256, 2) grouped_pack_kernel(const Inst *insts,
         const float *tile = reinterpret_cast<const float *>(stage_of(it));
         uint8_t *const *dst = cur.op ? cur.I->pb : cur.I->pa;
 #pragma unroll
-        for (int pass = 0; pass < kPackRows * (kBK / 8) / 256; ++pass) {
+        for (int pass = 0; pass < kPackRows * (kPackBK / 8) / 256; ++pass) {
             const int e = pass * 256 + tid;
             // 8 threads per row (coalesced 128-byte runs of pieces), 4 rows per warp
             const int r = e >> 3, c = e & 7;
@@ -231,8 +245,8 @@ __global__ void __launch_bounds__(256, 2) grouped_pack_kernel(const Inst *insts,
             if (!cur.transposed) {
                 // the upper four threads read their second half first: no bank conflicts
                 const int h = (c >> 2) & 1;
-                const float4 u = *reinterpret_cast<const float4 *>(tile + r * kBK + c * 8 + 4 * h);
-                const float4 v = *reinterpret_cast<const float4 *>(tile + r * kBK + c * 8 + 4 * (h ^ 1));
+                const float4 u = *reinterpret_cast<const float4 *>(tile + r * kPackBK + c * 8 + 4 * h);
+                const float4 v = *reinterpret_cast<const float4 *>(tile + r * kPackBK + c * 8 + 4 * (h ^ 1));
                 const float4 lo = h ? v : u, hi = h ? u : v;
                 x[0] = lo.x, x[1] = lo.y, x[2] = lo.z, x[3] = lo.w, x[4] = hi.x, x[5] = hi.y, x[6] = hi.z, x[7] = hi.w;
             } else {
@@ -286,7 +300,7 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
     using L = GLayoutOf<MODE, PAIR>;
     using MD = tcg::Mode<MODE>;
     constexpr int S = L::STAGES;
-    static_assert(L::BK == kBK, "grouped engine stages BF16 slices of 64");
+    static_assert(L::BK == kBK, "grouped engine stages BF16 slices of kBK");
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     __shared__ __align__(8) uint64_t full[S], empty[S], tfull[2], tempty[2], mma_done;
@@ -552,21 +566,21 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
                     const int row = row_off + quarter * 32 + rs * 16 + (lane >> 2) + 8 * rr;
                     if (row >= R->rows) continue;
                     float *cp = R->C + (int64_t)row * R->ldc + half * hw;
-                    // four 8-column groups at a time: their loads of C
+                    // kEpiBatch 8-column groups at a time: their loads of C
                     // (beta != 0) are issued together, then their stores
 #pragma unroll
-                    for (int g0 = 0; g0 < 16; g0 += 4) {
+                    for (int g0 = 0; g0 < 16; g0 += kEpiBatch) {
                         if (g0 >= ngroups) break;
-                        float2 c2[4];
+                        float2 c2[kEpiBatch];
 #pragma unroll
-                        for (int q = 0; q < 4; ++q) {
+                        for (int q = 0; q < kEpiBatch; ++q) {
                             const int col = (g0 + q) * 8 + cl;
                             c2[q] = make_float2(0.0f, 0.0f);
                             if (beta != 0.0f && vec_ok && col + 1 < ncols)
                                 c2[q] = *reinterpret_cast<const float2 *>(cp + col);
                         }
 #pragma unroll
-                        for (int q = 0; q < 4; ++q) {
+                        for (int q = 0; q < kEpiBatch; ++q) {
                             const int col = (g0 + q) * 8 + cl;
                             const int idx = (rs * 16 + g0 + q) * 4 + 2 * rr;
                             if (col >= ncols) continue;
@@ -723,11 +737,11 @@ static int resolve_instance(const gatlas_grouped_instance &in, int slot, InstPla
     o->bn = bn;
     o->mt = (int)((in.m + grp::BM - 1) / grp::BM);
     o->nt = (int)((in.n + bn - 1) / bn);
-    o->kt = (int)((in.k + grp::kBK - 1) / grp::kBK);
+    o->kt = (int)((in.k + grp::kPackBK - 1) / grp::kPackBK);
     if (in.m == 0 || in.n == 0) o->mt = o->nt = 0;
     if (o->mt > 65535 || o->kt > (1 << 24)) return set_error(GATLAS_ERR_INVALID, "grouped: instance too large");
-    o->a_piece = round_up((size_t)o->mt * o->kt * grp::kATileBytes, 1024);
-    o->b_piece = round_up((size_t)o->nt * o->kt * bn * grp::kRowBytes, 1024);
+    o->a_piece = round_up((size_t)o->mt * o->kt * grp::BM * grp::kPackRowBytes, 1024);
+    o->b_piece = round_up((size_t)o->nt * o->kt * bn * grp::kPackRowBytes, 1024);
     return GATLAS_OK;
 }
 
@@ -802,7 +816,7 @@ int grouped_build(int engine, const gatlas_grouped_instance *in, int32_t count, 
         // tile (read too when beta != 0), plus a fixed per-tile overhead
         // (a pair tile: both CTAs' halves, as one unit of its cluster's time)
         const int64_t c_bytes = (int64_t)step_m * grp::BM * o.bn * 4 * ((q.gemm && q.beta != 0.0) ? 2 : 1);
-        const int64_t cost = (int64_t)o.kt * t->np * (step_m * grp::BM + o.bn) * grp::kRowBytes + c_bytes + 16384;
+        const int64_t cost = (int64_t)o.kt * t->np * (step_m * grp::BM + o.bn) * grp::kPackRowBytes + c_bytes + 16384;
         // grouped raster inside the instance: 16 tile rows per group, so the
         // tiles that run at the same time share A and B rows through L2
         for (int g0 = 0; g0 < o.mt; g0 += 16)
@@ -811,12 +825,12 @@ int grouped_build(int engine, const gatlas_grouped_instance *in, int32_t count, 
                 grp::TileRec r;
                 std::memset(&r, 0, sizeof(r));
                 for (int j = 0; j < t->np && pb; ++j) {
-                    r.a[j] = I.pa[j] + (size_t)tm * o.kt * grp::kATileBytes;
-                    r.b[j] = I.pb[j] + (size_t)tn * o.kt * o.bn * grp::kRowBytes;
+                    r.a[j] = I.pa[j] + (size_t)tm * o.kt * grp::BM * grp::kPackRowBytes;
+                    r.b[j] = I.pb[j] + (size_t)tn * o.kt * o.bn * grp::kPackRowBytes;
                 }
                 r.C = q.c + (int64_t)tm * grp::BM * o.ldc + (int64_t)tn * o.bn;
                 r.ldc = o.ldc;
-                r.kt = o.kt;
+                r.kt = o.kt * grp::kSlicesPerItem;  // contraction K slices
                 r.bn = o.bn;
                 r.rows = (int32_t)std::min<int64_t>(step_m * grp::BM, o.M - (int64_t)tm * grp::BM);
                 r.cols = (int32_t)std::min<int64_t>(o.bn, o.N - (int64_t)tn * o.bn);

@@ -21,18 +21,18 @@ struct Inst {
     uint8_t *pa[2], *pb[2];  // packed pieces
     float *C;
     int64_t M, N, K, lda, ldb, ldc;
-    int32_t ta, tb, gemm, bn, mt, nt, kt, pad;
+    int32_t ta, tb, gemm, bn, mt, nt, kt, pad;  // kt: pack items (64 K elements) per row block
     float alpha, beta;
 };
 
 // Self-contained record of one output tile, in the order its CTA runs it:
 // the producer, the MMA issuer and the epilogue read nothing else.
 struct TileRec {
-    const uint8_t *a[2];  // piece tiles of this row block: [kt][128 rows x 64 B]
-    const uint8_t *b[2];  // piece tiles of this column block: [kt][bn rows x 64 B]
+    const uint8_t *a[2];  // piece tiles of this row block: [kt][128 rows x one K slice]
+    const uint8_t *b[2];  // piece tiles of this column block: [kt][bn rows x one K slice]
     float *C;             // C at the tile's origin
     int64_t ldc;
-    int32_t kt, bn, rows, cols;  // valid rows / columns of the tile
+    int32_t kt, bn, rows, cols;  // K slices; tile width; valid rows / columns of the tile
     float alpha, beta;
     int32_t gemm, pad;
 };

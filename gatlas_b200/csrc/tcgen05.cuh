@@ -273,12 +273,6 @@ __device__ __forceinline__ uint64_t l2_policy_evict_last() {
     return pol;
 }
 
-__device__ __forceinline__ uint64_t l2_policy_evict_first() {
-    uint64_t pol;
-    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
-    return pol;
-}
-
 // tma_load_3d / tma_load_3d_pair with an L2 eviction priority.
 __device__ __forceinline__ void tma_load_3d_hint(void *smem_dst, const void *tmap, int32_t x, int32_t y, int32_t z,
                                                  uint64_t *bar, uint64_t policy) {

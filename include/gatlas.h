@@ -208,6 +208,9 @@ int gatlas_matmul_f32_host(const gatlas_matmul_desc *d, const float *A, const fl
  * tiles in flight cover a block of that height, whose operands share L2.
  * "host_block_rows": rows of A per pipelined block of gatlas_matmul_f32_host,
  * a multiple of 256 (default 512).
+ * "tc_l2_hint": 1 (default) loads A's tiles in the persistent tensor-core
+ * contraction with an evict-last L2 priority (A is reused by every tile
+ * column of a raster group); 0 loads them plainly.  Results are identical.
  * "grouped_pair": how grouped contractions tile C.  0 (default): 128-row
  * tiles on single CTAs.  1: 256-row tiles on CTA pairs (an instance's row
  * blocks two at a time, each CTA staging half of the B tile; the second half

@@ -82,9 +82,9 @@ def test_options_round_trip_without_a_device():
         g.set_option("no_such_option", 1)
     with pytest.raises(g.GatlasError, match="0, 1 or 2"):
         g.set_option("tc_pair", 3)
-    assert g.get_option("tc_l2_hint") == 0
-    with pytest.raises(g.GatlasError, match="0, 1 or 2"):
-        g.set_option("tc_l2_hint", 3)
+    assert g.get_option("tc_l2_hint") == 1
+    with pytest.raises(g.GatlasError, match="0 or 1"):
+        g.set_option("tc_l2_hint", 2)
     assert g.get_option("grouped_pair") == 0
     g.set_option("grouped_pair", 1)
     try:
