@@ -56,9 +56,9 @@ def _peaks():
 
 
 # DRAM bytes (read + write) per launch of the split3 contraction at 8192^3
-# (persistent kernel on CTA pairs), from an ncu capture of the full-size
-# launch (profiles/tc_gemm_persistent_split3_pair_8192.md)
-TC_TRAFFIC_BYTES = 3.181e9 + 0.264e9
+# (persistent kernel on CTA pairs, A's loads evict-last), from an ncu capture
+# of the full-size launch (profiles/tc_gemm_persistent_split3_pair_8192.md)
+TC_TRAFFIC_BYTES = 2.542e9 + 0.263e9
 TC_KERNEL = "tc_gemm_persistent_kernel<split3, CTA pair>"
 
 # nominal FP32 SIMT peak: 148 SMs x 128 FP32 lanes x 2 flop x 1.965 GHz
