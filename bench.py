@@ -686,7 +686,7 @@ def _summary(o: dict) -> dict:
     cb = o.get("cpu_baseline") or {}
     if cb:
         sm["cpu"] = {"tflops": r(cb["value"], 4), "kind": cb["kind"], "cores": cb["cores"],
-                     "secondary": {k: r(v, 3) for k, v in (cb.get("secondary") or {}).items()}}
+                     "secondary": {k: float(f"{v:.4g}") for k, v in (cb.get("secondary") or {}).items()}}
     return sm
 
 
@@ -741,7 +741,8 @@ def _ref_sgemm_sample(R, seconds: float, threads: int):
 def _ref_secondary(R, threads: int) -> dict:
     """The reference's memory-bound kernels at the workload sizes (SAXPY
     n = 2^28 as 2^26 float4; SGEMV 16384^2, both layouts, buffer and image)
-    and its SGEMM 1024^3 point, timed once each after one untimed call."""
+    and its SGEMM 1024^3 point, timed once each after one untimed call; and
+    the naive host loop at 1024^3 on one thread."""
     import numpy as np
 
     import oracle
@@ -770,6 +771,11 @@ def _ref_secondary(R, threads: int) -> dict:
     t0 = time.perf_counter()
     R.run("bench_sgemm_1024", A1, B1, C1, threads=threads)
     out["sgemm_1024_tflops"] = 2.0 * m ** 3 / (time.perf_counter() - t0) / 1e12
+    # the reference's naive host check loop (KernelMatmulBuffer.hpp:124-143,
+    # restated in the oracle), one thread as the reference runs it
+    t0 = time.perf_counter()
+    oracle.matmul(A1, B1, m, m, m, mode=oracle.REFHOST, threads=1)
+    out["sgemm_1024_host_loop_tflops"] = 2.0 * m ** 3 / (time.perf_counter() - t0) / 1e12
     return out
 
 
