@@ -21,10 +21,14 @@ constexpr int BM = 128, BN = 256;
 // One-product BF16 accumulates all of K in TMEM (kSegAll): the tensor core's
 // FP32 accumulation error stays far below BF16's own input rounding (2^-9),
 // and without promotion a 256 x 256 tile fits one CTA.  FP8 accumulates runs
-// of at most 4 equally scaled 128-deep blocks.
+// of at most 16 equally scaled 128-deep blocks (K = 2048): at 8192^3 on
+// sign * 2^e operands, which E4M3 holds exactly, the normwise error is
+// 1.2e-6 (3.2e-7 with runs of 4, below SIMT FP32's 1.6e-6 either way), on
+// uniform operands E4M3's own rounding (0.033) is unchanged, and the
+// contraction takes 0.490 ms instead of 0.517.
 constexpr int kSegAll = 1 << 30;
 __host__ __device__ constexpr int default_seg_kblocks(int mode) {
-    return mode == 0 ? kSegAll : 4;
+    return mode == 0 ? kSegAll : mode == 3 ? 16 : 4;
 }
 // FP8: most 128-deep blocks per tile (K <= 131072).
 constexpr int kMaxFp8Blocks = 1024;

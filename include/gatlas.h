@@ -142,7 +142,7 @@ int gatlas_matvec_f32_noalloc(const gatlas_matvec_desc *d, const float *A, const
  * for TC_SPLIT3 and K = 128 for TC_SPLIT6.
  * GATLAS_ENGINE_TC_FP8 quantises each operand to E4M3 with one power-of-two
  * FP32 scale per 128 x 128 block (the smallest power of two s with
- * amax / s <= 448); runs of up to `extra` (0 selects 4) 128-deep blocks
+ * amax / s <= 448); runs of up to `extra` (0 selects 16) 128-deep blocks
  * whose scale products sa * sb are equal accumulate in TMEM and are promoted
  * scaled once, exactly (powers of two), K <= 131072; its
  * tc_prepare workspace holds [A codes][B codes][A scales][B scales][plan],
