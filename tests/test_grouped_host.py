@@ -58,7 +58,7 @@ def test_create_rejects_bad_arguments_before_device_work():
 
 
 @pytest.mark.parametrize("engine", ["tc_bf16", "tc_split3"])
-def test_create_asks_for_exactly_the_queried_workspace(engine):
+def test_create_asks_for_exactly_the_queried_workspace(engine, no_cuda_device):
     """A caller's workspace one byte short of the query is rejected with the
     size create needs, which is the query's; an unaligned one is rejected too
     (both before any device work)."""

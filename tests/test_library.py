@@ -131,7 +131,7 @@ def test_matvec_workspace_query_covers_the_image_engine(M, N):
 @pytest.mark.parametrize("engine", ["tc_bf16", "tc_split3", "tc_split6", "tc_fp8"])
 @pytest.mark.parametrize("M,N,K,ta,tb,batch", [(1000, 700, 333, 0, 0, 1), (4096, 4096, 4096, 1, 1, 1),
                                                (129, 257, 1000, 0, 1, 3), (16, 16, 16, 1, 0, 65535)])
-def test_tc_prepare_asks_for_exactly_the_queried_workspace(engine, M, N, K, ta, tb, batch):
+def test_tc_prepare_asks_for_exactly_the_queried_workspace(engine, M, N, K, ta, tb, batch, no_cuda_device):
     """tc_prepare rejects a workspace one byte short of gatlas_matmul_workspace_size
     with the size it needs, which is the query's (before any device work)."""
     need = g.matmul_workspace_size(M, N, K, engine, ta, tb, batch)
