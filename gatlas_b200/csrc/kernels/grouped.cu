@@ -50,12 +50,16 @@ constexpr uint32_t kRowBytes = 128;       // one contraction K slice of one row 
 constexpr int kBK = kRowBytes / 2;        // BF16 elements per contraction K slice
 constexpr int kSlicesPerItem = (int)(kPackRowBytes / kRowBytes);
 constexpr uint32_t kATileBytes = BM * kRowBytes;
-constexpr int kDrainWarps = 8;
+constexpr int kDrainWarps = 8;            // a multiple of 4: kDrainParts warps per TMEM lane quarter
 constexpr int kThreads = 32 * (2 + kDrainWarps);
+constexpr int kDrainParts = kDrainWarps / 4;          // column parts of a tile per lane quarter
+constexpr int kPartGroups = 256 / kDrainParts / 8;    // 8-column groups in a part of the widest tile
+constexpr int kAccRegs = 2 * kPartGroups * 4;         // accumulator registers per drain thread
 constexpr uint32_t kTmemCols = 512;       // two accumulators of up to 256 columns
 constexpr uint64_t kWaitNs = 2000000000ull;
 constexpr int kPackRows = 128;            // rows per pack item
 constexpr int kEpiBatch = 8;              // 8-column groups of C loaded together by the epilogue
+static_assert(kDrainWarps % 4 == 0 && kPartGroups % kEpiBatch == 0, "drain layout");
 // The grouped engine stages 64-byte K slices (its packed tiles carry the
 // 64-byte swizzle), so that a ring of 48 KiB stages holds four split3 K slices
 // of a 128 x 256 tile, and promotes after the same K as the single-instance
@@ -484,7 +488,7 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
         __syncwarp();
     } else {
         // ---- drain + epilogue ----
-        const int quarter = warp & 3, half = (warp - 2) >> 2;
+        const int quarter = warp & 3, part = (warp - 2) >> 2;
         const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
         const int row_off = PAIR ? (int)rank * 128 : 0;  // a pair CTA's rows of the 256-row tile
         const uint32_t tempty_leader = PAIR ? tc::mapa_shared(smem_u32(&tempty[0]), 0) : 0u;
@@ -493,27 +497,27 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
         for (int t = t_begin; t < t_end && ok; ++t) {
             const TileRec *R = p.tiles + t;
             const int bn = R->bn, kt = R->kt;
-            const int hw = bn >> 1;            // columns of this warp's half
+            const int hw = bn / kDrainParts;   // columns of this warp's part of the tile
             const int nseg = (kt + p.seg_kblocks - 1) / p.seg_kblocks;
             // Accumulator fragments in the 16x256b layout: for row slab rs (TMEM
             // lanes 16*rs .. 16*rs+15 of this warp's quarter) and column group
-            // cg (8 columns), acc[(rs*16 + cg)*4 + e] holds row
+            // cg (8 columns), acc[(rs*kPartGroups + cg)*4 + e] holds row
             // 16*rs + lane/4 (e = 0, 1) or 16*rs + lane/4 + 8 (e = 2, 3), column
-            // 8*cg + 2*(lane%4) + (e & 1) of this warp's half of the tile.  Four
+            // 8*cg + 2*(lane%4) + (e & 1) of this warp's part of the tile.  Four
             // neighbouring lanes then hold 32 contiguous bytes of one row of C,
             // so each store request covers whole sectors of eight rows.
-            float acc[128];
+            float acc[kAccRegs];
 #pragma unroll
-            for (int j = 0; j < 128; ++j) acc[j] = 0.0f;
-            const int ngroups = hw >> 3;         // 8-column groups of this warp's half: 4, 8 or 16
+            for (int j = 0; j < kAccRegs; ++j) acc[j] = 0.0f;
+            const int ngroups = hw >> 3;         // 8-column groups of this warp's part: 2 to kPartGroups
             {
                 // C is read by the epilogue (beta != 0): pull this warp's rows
                 // of it into L2 while the tile's MMAs run
                 const int r = row_off + quarter * 32 + lane;
                 if (R->gemm && R->beta != 0.0f && r < R->rows) {
-                    const int left = R->cols - half * hw;
+                    const int left = R->cols - part * hw;
                     const int ncols = left < hw ? left : hw;
-                    const char *row = reinterpret_cast<const char *>(R->C + (int64_t)r * R->ldc + half * hw);
+                    const char *row = reinterpret_cast<const char *>(R->C + (int64_t)r * R->ldc + part * hw);
                     for (int off = 0; off < ncols * 4; off += 128)
                         asm volatile("prefetch.global.L2 [%0];" ::"l"(row + off));
                 }
@@ -527,20 +531,32 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
                     break;
                 }
                 tc::fence_after_sync();
-                const uint32_t col_base = tmem + lane_base + (uint32_t)(b * 256 + half * hw);
+                const uint32_t col_base = tmem + lane_base + (uint32_t)(b * 256 + part * hw);
 #pragma unroll
                 for (int rs = 0; rs < 2; ++rs) {
+                    const uint32_t slab = col_base + ((uint32_t)(rs * 16) << 16);
+                    if (ngroups >= 4) {
 #pragma unroll
-                    for (int c = 0; c < 4; ++c) {   // 32 columns per load
-                        if (c * 4 < ngroups) {
-                            uint32_t r[16];
-                            tc::tmem_ld_16x256b_x4(col_base + ((uint32_t)(rs * 16) << 16) + (uint32_t)(c * 32), r);
-                            tc::tmem_ld_wait();
+                        for (int c = 0; c < kPartGroups / 4; ++c) {   // 32 columns per load
+                            if (c * 4 < ngroups) {
+                                uint32_t r[16];
+                                tc::tmem_ld_16x256b_x4(slab + (uint32_t)(c * 32), r);
+                                tc::tmem_ld_wait();
 #pragma unroll
-                            for (int j = 0; j < 16; ++j) {
-                                const int idx = (rs * 16 + c * 4) * 4 + j;
-                                acc[idx] = __fadd_rn(acc[idx], __uint_as_float(r[j]));
+                                for (int j = 0; j < 16; ++j) {
+                                    const int idx = (rs * kPartGroups + c * 4) * 4 + j;
+                                    acc[idx] = __fadd_rn(acc[idx], __uint_as_float(r[j]));
+                                }
                             }
+                        }
+                    } else {   // a 16-column part (64-wide tiles split four ways)
+                        uint32_t r[8];
+                        tc::tmem_ld_16x256b_x2(slab, r);
+                        tc::tmem_ld_wait();
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const int idx = rs * kPartGroups * 4 + j;
+                            acc[idx] = __fadd_rn(acc[idx], __uint_as_float(r[j]));
                         }
                     }
                 }
@@ -552,12 +568,12 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
                 }
             }
             if (!ok || abort_flag) break;
-            const int left = R->cols - half * hw;
-            const int ncols = left < hw ? left : hw;  // valid columns of this half
+            const int left = R->cols - part * hw;
+            const int ncols = left < hw ? left : hw;  // valid columns of this part
             const bool gemm = R->gemm != 0;
             const float alpha = R->alpha, beta = gemm ? R->beta : 0.0f;
             const bool vec_ok = ((R->ldc & 1) == 0) && ((reinterpret_cast<uintptr_t>(R->C) & 7) == 0) &&
-                                ((half * hw) % 2 == 0);
+                                ((part * hw) % 2 == 0);
             const int cl = 2 * (lane & 3);
 #pragma unroll
             for (int rs = 0; rs < 2; ++rs) {
@@ -565,11 +581,11 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
                 for (int rr = 0; rr < 2; ++rr) {
                     const int row = row_off + quarter * 32 + rs * 16 + (lane >> 2) + 8 * rr;
                     if (row >= R->rows) continue;
-                    float *cp = R->C + (int64_t)row * R->ldc + half * hw;
+                    float *cp = R->C + (int64_t)row * R->ldc + part * hw;
                     // kEpiBatch 8-column groups at a time: their loads of C
                     // (beta != 0) are issued together, then their stores
 #pragma unroll
-                    for (int g0 = 0; g0 < 16; g0 += kEpiBatch) {
+                    for (int g0 = 0; g0 < kPartGroups; g0 += kEpiBatch) {
                         if (g0 >= ngroups) break;
                         float2 c2[kEpiBatch];
 #pragma unroll
@@ -582,7 +598,7 @@ __global__ void __launch_bounds__(kThreads, 1) grouped_gemm_kernel(Params p) {
 #pragma unroll
                         for (int q = 0; q < kEpiBatch; ++q) {
                             const int col = (g0 + q) * 8 + cl;
-                            const int idx = (rs * 16 + g0 + q) * 4 + 2 * rr;
+                            const int idx = (rs * kPartGroups + g0 + q) * 4 + 2 * rr;
                             if (col >= ncols) continue;
                             if (vec_ok && col + 1 < ncols) {
                                 float2 v;
