@@ -133,6 +133,20 @@ __device__ __forceinline__ void img_load(void *dst, const TmapBlob *map, int32_t
 __device__ __forceinline__ float img_fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double img_fma(double a, double b, double c) { return __fma_rn(a, b, c); }
 
+// Two round-to-nearest fused multiply-adds in one packed instruction
+// (fma.rn.f32x2, sm_100): d0 = a*b0 + d0 and d1 = a*b1 + d1, each exactly
+// what __fmaf_rn gives.
+__device__ __forceinline__ void img_fma2(float &d0, float &d1, float a, float b0, float b1) {
+    asm("{.reg .b64 pa, pb, pd;\n\t"
+        "mov.b64 pa, {%2, %2};\n\t"
+        "mov.b64 pb, {%3, %4};\n\t"
+        "mov.b64 pd, {%0, %1};\n\t"
+        "fma.rn.f32x2 pd, pa, pb, pd;\n\t"
+        "mov.b64 {%0, %1}, pd;}"
+        : "+f"(d0), "+f"(d1)
+        : "f"(a), "f"(b0), "f"(b1));
+}
+
 template <typename T, bool TA, bool TB, int GH, int GW, int BH, int BW>
 __global__ void __launch_bounds__(GH *GW, (GH * GW <= 256) ? 2 : 1)
     gemm_image_kernel(const __grid_constant__ TmapBlob mapA, const __grid_constant__ TmapBlob mapB, ImgArgs<T> a) {
@@ -232,10 +246,19 @@ __global__ void __launch_bounds__(GH *GW, (GH * GW <= 256) ? 2 : 1)
 #pragma unroll
                 for (int j = 0; j < BW; ++j) bf[j] = Bk[kk * PB + tx * BW + j];
             }
+            // FP32 column pairs in one packed instruction: the same fused
+            // multiply-add chain per element, half the FMA instructions
+            if constexpr (sizeof(T) == 4 && BW % 2 == 0) {
 #pragma unroll
-            for (int i = 0; i < BH; ++i)
+                for (int i = 0; i < BH; ++i)
 #pragma unroll
-                for (int j = 0; j < BW; ++j) acc[i][j] = img_fma(af[i], bf[j], acc[i][j]);
+                    for (int j = 0; j < BW; j += 2) img_fma2(acc[i][j], acc[i][j + 1], af[i], bf[j], bf[j + 1]);
+            } else {
+#pragma unroll
+                for (int i = 0; i < BH; ++i)
+#pragma unroll
+                    for (int j = 0; j < BW; ++j) acc[i][j] = img_fma(af[i], bf[j], acc[i][j]);
+            }
         }
         __syncthreads();
     }
