@@ -52,6 +52,7 @@ struct InstPlan {
 struct GroupedTables {
     int engine = 0, np = 1, mode = 0;
     bool pair = false;  // 256-row tiles on CTA pairs; `grid` and `cta` count clusters
+    bool vec = false;   // every instance's C takes 8-byte vector accesses
     std::vector<InstPlan> ip;
     std::vector<grp::Inst> inst;
     std::vector<int64_t> seg;

@@ -69,6 +69,35 @@ def test_grouped_equals_single_instance_engine(cuda, engine):
     plan.close()
 
 
+# every C takes 8-byte vector accesses (even n): the launch runs the
+# vector-only epilogue; ragged tiles in both dimensions, beta in {0, 1}
+EVEN_SHAPES = [
+    (128, 256, 64, 0, 0, 0, 1.0, 0.0, 0), (200, 300, 100, 0, 1, 1, 0.5, 1.0, 0), (33, 18, 5, 1, 0, 1, 1.0, 1.0, 64),
+    (257, 130, 520, 1, 1, 1, 2.0, 0.0, 128), (16, 4000, 48, 0, 0, 1, 1.5, 1.0, 256), (1000, 16, 700, 1, 0, 0, 1.0, 0.0, 0),
+    (130, 70, 90, 1, 1, 1, 0.75, 1.0, 128), (96, 1022, 33, 1, 0, 1, 1.0, 1.0, 0), (300, 500, 0, 0, 0, 1, 1.0, 0.5, 0),
+]
+
+
+@pytest.mark.parametrize("engine", ["tc_bf16", "tc_split3"])
+@pytest.mark.parametrize("pair", [0, 1])
+def test_vector_epilogue_equals_single_instance_engine(cuda, engine, pair, pair_option):
+    g.set_option("grouped_pair", pair)
+    inst = _make(cuda, EVEN_SHAPES, seed=11)
+    plan = g.Grouped(inst, engine=engine)
+    plan.prepare().run()
+    got = _results(inst)
+    _reset(inst)
+    plan.run_each()
+    want = _results(inst)
+    for q, x, y in zip(inst, got, want):
+        assert np.array_equal(x, y), (q["m"], q["n"], q["k"])
+        if q["m"] and q["n"]:
+            ref = oracle.matmul(q["hA"], q["hB"], q["m"], q["n"], q["k"], q["trans_a"], q["trans_b"], mode=oracle.F64,
+                                gemm=q["gemm"], Cin=q["hC0"], alpha=q["alpha"], beta=q["beta"])
+            assert oracle.normwise_error(x, ref) <= BUDGET[engine]
+    plan.close()
+
+
 @pytest.fixture
 def pair_option():
     old = g.get_option("grouped_pair")
