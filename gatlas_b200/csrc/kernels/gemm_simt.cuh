@@ -227,6 +227,47 @@ __global__ void __launch_bounds__(GH *GW, min_blocks<T, GH * GW, BH * BW>())
         }
     };
 
+
+    // L2 prefetch of the operand vectors of a later K step: it holds no
+    // registers, and the register-staged loads of that step then hit L2
+    // instead of waiting on DRAM
+    auto prefetch_tile = [&](int64_t k0) {
+#pragma unroll
+        for (int it = 0; it < TT::LA; ++it) {
+            const int v = tid + it * NT;
+            if (v < TT::A_VECS) {
+                const T *ptr = nullptr;
+                if constexpr (!TA) {
+                    const int kv = v % (BK / VL), m = v / (BK / VL);
+                    const int64_t gr = m0 + m, gc = k0 + kv * VL;
+                    if (gr < a.M && gc < a.K) ptr = A + gr * a.lda + gc;
+                } else {
+                    const int mv = v % (BM / VL), k = v / (BM / VL);
+                    const int64_t gr = k0 + k, gc = m0 + mv * VL;
+                    if (gr < a.K && gc < a.M) ptr = A + gr * a.lda + gc;
+                }
+                if (ptr) asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
+            }
+        }
+#pragma unroll
+        for (int it = 0; it < TT::LB; ++it) {
+            const int v = tid + it * NT;
+            if (v < TT::B_VECS) {
+                const T *ptr = nullptr;
+                if constexpr (!TB) {
+                    const int nv = v % (BN / VL), k = v / (BN / VL);
+                    const int64_t gr = k0 + k, gc = n0 + nv * VL;
+                    if (gr < a.K && gc < a.N) ptr = B + gr * a.ldb + gc;
+                } else {
+                    const int kv = v % (BK / VL), n = v / (BK / VL);
+                    const int64_t gr = n0 + n, gc = k0 + kv * VL;
+                    if (gr < a.N && gc < a.K) ptr = B + gr * a.ldb + gc;
+                }
+                if (ptr) asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
+            }
+        }
+    };
+
     T acc[BH][BW];
 #pragma unroll
     for (int i = 0; i < BH; ++i)
@@ -242,6 +283,12 @@ __global__ void __launch_bounds__(GH *GW, min_blocks<T, GH * GW, BH * BW>())
 
     for (int64_t kt = 0; kt < KT; ++kt) {
         const int cur = (int)(kt & 1);
+        // two K steps ahead, for FP32 points that run two CTAs per SM under
+        // the 128-register cap (8192^3 default point 47.9 -> 50.6 TFLOP/s);
+        // one-CTA points (8x16 x 16x8: 47.5 -> 44.7) and FP64 (21.1 -> 20.4
+        // at 4096^3) ran slower with it and go without
+        if constexpr (sizeof(T) == 4 && min_blocks<T, NT, BH * BW>() > 1)
+            if (kt + 2 < KT) prefetch_tile((kt + 2) * BK);
         if (kt + 1 < KT) load_tile((kt + 1) * BK);
 #pragma unroll
         for (int kk = 0; kk < BK; ++kk) {
